@@ -1,0 +1,664 @@
+// C ABI of libgat (include/gat.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <chrono>
+#include <climits>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/gat.h"
+#include "engine.hpp"
+#include "gat_internal.hpp"
+#include "graph.hpp"
+
+using namespace gat;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(GAT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int copy_out(const std::string &s, char *buf, size_t cap, size_t *needed) {
+    if (needed) *needed = s.size() + 1;
+    if (!buf) return GAT_OK;
+    if (cap < s.size() + 1) return fail(GAT_ERR_ARGUMENT, "buffer too small");
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return GAT_OK;
+}
+
+}  // namespace
+
+struct gat_pattern {
+    Pattern p;
+};
+
+struct gat_schedule {
+    int mode = 0;
+    bool trivial = false;  // n <= 2: counted on the host
+    Pattern pattern;
+    RefSchedule ref;
+    PlanInfo plan;
+    std::string json;
+};
+
+struct DevCopy {
+    int64_t *off = nullptr;
+    int32_t *adj = nullptr;
+    int64_t *lo_off = nullptr;
+    int64_t lo_total = 0;
+    int32_t max_degree = 0;
+    bool ready = false;
+    void release() {
+        cudaFree(off);
+        cudaFree(adj);
+        cudaFree(lo_off);
+        *this = DevCopy{};
+    }
+};
+
+struct gat_graph {
+    HostGraph host;
+    DevCopy dev;          // ids as given
+    DevCopy dev_ordered;  // relabelled by decreasing degree
+    int device = -1;
+    ~gat_graph() {
+        dev.release();
+        dev_ordered.release();
+    }
+};
+
+struct gat_executor {
+    gat_config cfg{};
+    int device = 0;
+    int sms = 0;
+    int32_t *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    DevCounters *ctr = nullptr;
+    DevCounters *host_ctr = nullptr;  // pinned
+    GatPlan *d_plan = nullptr;
+    GatPlan *h_plan = nullptr;  // pinned
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~gat_executor() {
+        cudaFree(scratch);
+        cudaFree(ctr);
+        cudaFree(d_plan);
+        cudaFreeHost(host_ctr);
+        cudaFreeHost(h_plan);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+extern "C" {
+
+const char *gat_last_error(void) { return g_last_error.c_str(); }
+const char *gat_version(void) { return "libgat 0.1 (sm_100a)"; }
+
+// ------------------------------------------------------------ pattern
+
+int gat_pattern_from_adj(const char *adj, gat_pattern **out) {
+    if (!adj || !out) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    Pattern p;
+    if (!Pattern::parse(adj, p))
+        return fail(GAT_ERR_PATTERN,
+                    "pattern must be n*n characters '0'/'1' with 1 <= n <= 10");
+    *out = new gat_pattern{p};
+    return GAT_OK;
+}
+
+int gat_pattern_vertices(const gat_pattern *p) { return p ? p->p.n : 0; }
+
+int gat_pattern_automorphisms(const gat_pattern *p, int64_t *out) {
+    if (!p || !out) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *out = (int64_t)automorphisms(p->p).size();
+    return GAT_OK;
+}
+
+int gat_pattern_adjacency(const gat_pattern *p, char *buf, size_t cap) {
+    if (!p) return fail(GAT_ERR_ARGUMENT, "null argument");
+    return copy_out(p->p.adjacency(), buf, cap, nullptr);
+}
+
+void gat_pattern_free(gat_pattern *p) { delete p; }
+
+int gat_enumerate_patterns(int n, char *buf, size_t cap, size_t *needed) {
+    if (n < 1 || n > 6) return fail(GAT_ERR_ARGUMENT, "n must be in [1, 6]");
+    std::string s;
+    for (auto &x : enumerate_connected_patterns(n)) {
+        if (!s.empty()) s += '\n';
+        s += x;
+    }
+    return copy_out(s, buf, cap, needed);
+}
+
+// ----------------------------------------------------------- schedule
+
+int gat_schedule_build(const gat_pattern *p, int mode,
+                       const gat_graph *stats_graph, gat_schedule **out) {
+    if (!p || !out) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (mode != GAT_MODE_EXACT && mode != GAT_MODE_REF_COMPAT)
+        return fail(GAT_ERR_ARGUMENT, "unknown mode");
+    auto s = std::make_unique<gat_schedule>();
+    s->mode = mode;
+    s->pattern = p->p;
+    std::string err;
+    if (mode == GAT_MODE_REF_COMPAT) {
+        if (!build_ref_schedule(p->p, s->ref, &err)) return fail(GAT_ERR_PATTERN, err);
+        s->json = ref_schedule_json(s->ref);
+        if (p->p.n <= 2) {
+            s->trivial = true;
+        } else if (!plan_from_ref(s->ref, s->plan, &err)) {
+            // Keep the schedule (it can be dumped) but mark it uncountable.
+            s->plan = PlanInfo{};
+            s->plan.summary = err;
+        }
+    } else {
+        if (p->p.n <= 2) {
+            if (!pattern_connected(p->p)) return fail(GAT_ERR_PATTERN, "pattern is not connected");
+            s->trivial = true;
+            s->json = "{\"mode\":\"exact\",\"trivial\":true}";
+        } else {
+            GraphStats gs;
+            if (stats_graph && stats_graph->host.V > 0) {
+                gs.v = stats_graph->host.V;
+                gs.e = stats_graph->host.E / 2;
+                gs.tri = std::max<int64_t>(1, gs.e / 10);
+            }
+            if (!plan_exact(p->p, gs, s->plan, &err)) return fail(GAT_ERR_PATTERN, err);
+            std::string perm, r;
+            for (size_t i = 0; i < s->plan.perm.size(); i++)
+                perm += (i ? "," : "") + std::to_string(s->plan.perm[i]);
+            for (size_t i = 0; i < s->plan.restrictions.size(); i++)
+                r += std::string(i ? "," : "") + "[" +
+                     std::to_string(s->plan.restrictions[i].first) + "," +
+                     std::to_string(s->plan.restrictions[i].second) + "]";
+            s->json = "{\"mode\":\"exact\",\"pattern\":\"" + p->p.adjacency() +
+                      "\",\"perm\":[" + perm + "],\"restrictions\":[" + r +
+                      "],\"basic_vertexes\":" + std::to_string(s->plan.plan.basic) +
+                      ",\"divisor\":" + std::to_string(s->plan.plan.divisor) +
+                      ",\"aut\":" + std::to_string(s->plan.aut) + "}";
+        }
+    }
+    *out = s.release();
+    return GAT_OK;
+}
+
+int gat_schedule_mode(const gat_schedule *s) { return s ? s->mode : -1; }
+
+int gat_schedule_dump(const gat_schedule *s, char *buf, size_t cap,
+                      size_t *needed) {
+    if (!s) return fail(GAT_ERR_ARGUMENT, "null argument");
+    return copy_out(s->json, buf, cap, needed);
+}
+
+int gat_schedule_plan(const gat_schedule *s, void *buf, size_t cap,
+                      size_t *needed) {
+    if (!s) return fail(GAT_ERR_ARGUMENT, "null argument");
+    if (needed) *needed = sizeof(GatPlan);
+    if (s->trivial || s->plan.plan.n == 0)
+        return fail(GAT_ERR_UNDEFINED, s->trivial ? "trivial schedule has no plan"
+                                                  : s->plan.summary);
+    if (!buf) return GAT_OK;
+    if (cap < sizeof(GatPlan)) return fail(GAT_ERR_ARGUMENT, "buffer too small");
+    std::memcpy(buf, &s->plan.plan, sizeof(GatPlan));
+    return GAT_OK;
+}
+
+void gat_schedule_free(gat_schedule *s) { delete s; }
+
+// ------------------------------------------------------------- config
+
+void gat_config_default(gat_config *c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->set_search_type = 64;
+    c->set_intersection_type = 0;
+    c->vertex_store_type = 0;
+    c->graph_backend_type = 0;
+    c->num_blocks = 256;
+    c->threads_per_block = 128;
+    c->threads_per_warp = 1;
+    c->max_regs = 32;
+    c->chunk = 16;
+    c->memory_budget = 0;
+}
+
+void gat_config_engine_default(gat_config *c) {
+    if (!c) return;
+    gat_config_default(c);
+    c->set_search_type = 0;
+    c->num_blocks = 0;
+    c->threads_per_block = 256;
+    c->threads_per_warp = 32;
+    c->max_regs = 64;
+    c->chunk = 8;
+}
+
+namespace {
+bool set_field(gat_config *c, const std::string &key, const std::string &val) {
+    auto ident = [&](int64_t &out) {
+        if (val == "Parallel" || val == "Array" || val == "InMemory") {
+            out = 0;
+            return true;
+        }
+        if (val == "Serial" || val == "Bitmap") {
+            out = 1;
+            return true;
+        }
+        if (val == "INT_MAX") {
+            out = INT32_MAX;
+            return true;
+        }
+        if (val.empty()) return false;
+        char *end = nullptr;
+        long long x = std::strtoll(val.c_str(), &end, 10);
+        if (*end != '\0') return false;
+        out = x;
+        return true;
+    };
+    std::string k = key.substr(key.rfind('.') + 1);
+    int64_t x = 0;
+    if (!ident(x)) return false;
+    auto i32 = [&](int32_t &f) {
+        if (x < INT32_MIN || x > INT32_MAX) return false;
+        f = (int32_t)x;
+        return true;
+    };
+    if (k == "set_search_type") return i32(c->set_search_type);
+    if (k == "set_intersection_type") return i32(c->set_intersection_type);
+    if (k == "vertex_store_type") return i32(c->vertex_store_type);
+    if (k == "graph_backend_type") return i32(c->graph_backend_type);
+    if (k == "num_blocks") return i32(c->num_blocks);
+    if (k == "threads_per_block") return i32(c->threads_per_block);
+    if (k == "threads_per_warp") return i32(c->threads_per_warp);
+    if (k == "max_regs") return i32(c->max_regs);
+    if (k == "chunk") return i32(c->chunk);
+    if (k == "memory_budget") {
+        c->memory_budget = x;
+        return true;
+    }
+    return true;  // unknown keys are ignored, like the C++ designated
+                  // initializer ignores nothing but the tuner may add fields
+}
+}  // namespace
+
+int gat_config_parse(const char *text, gat_config *c) {
+    if (!text || !c) return fail(GAT_ERR_ARGUMENT, "null argument");
+    std::string s(text);
+    size_t i = 0;
+    auto is_id = [](char ch) {
+        return std::isalnum((unsigned char)ch) || ch == '_' || ch == '.';
+    };
+    int found = 0;
+    while (i < s.size()) {
+        std::string key;
+        if (s[i] == '.' && i + 1 < s.size() &&
+            (std::isalpha((unsigned char)s[i + 1]) || s[i + 1] == '_')) {
+            size_t j = i + 1;
+            while (j < s.size() && (std::isalnum((unsigned char)s[j]) || s[j] == '_')) j++;
+            key = s.substr(i + 1, j - i - 1);
+            i = j;
+            while (i < s.size() && std::isspace((unsigned char)s[i])) i++;
+            if (i >= s.size() || s[i] != '=') continue;
+            i++;
+        } else if (s[i] == '"') {
+            size_t j = s.find('"', i + 1);
+            if (j == std::string::npos) break;
+            key = s.substr(i + 1, j - i - 1);
+            i = j + 1;
+            while (i < s.size() && std::isspace((unsigned char)s[i])) i++;
+            if (i >= s.size() || s[i] != ':') continue;
+            i++;
+        } else {
+            i++;
+            continue;
+        }
+        while (i < s.size() && std::isspace((unsigned char)s[i])) i++;
+        if (i < s.size() && s[i] == '{') continue;  // nested struct
+        std::string val;
+        if (i < s.size() && s[i] == '"') {
+            size_t j = s.find('"', i + 1);
+            if (j == std::string::npos) break;
+            val = s.substr(i + 1, j - i - 1);
+            i = j + 1;
+        } else {
+            size_t j = i;
+            while (j < s.size() && (is_id(s[j]) || s[j] == '-')) j++;
+            val = s.substr(i, j - i);
+            i = j;
+        }
+        if (!set_field(c, key, val))
+            return fail(GAT_ERR_CONFIG, "bad value '" + val + "' for " + key);
+        found++;
+    }
+    if (found == 0) return fail(GAT_ERR_CONFIG, "no configuration fields found");
+    return GAT_OK;
+}
+
+int gat_config_format(const gat_config *c, char *buf, size_t cap) {
+    if (!c) return fail(GAT_ERR_ARGUMENT, "null argument");
+    auto st = [](int v) {
+        return v == INT32_MAX ? std::string("2147483647") : std::to_string(v);
+    };
+    std::string s = "{.vertex_set_config = {.set_search_type = " +
+                     st(c->set_search_type) + ", .set_intersection_type = " +
+                     (c->set_intersection_type ? "Serial" : "Parallel") +
+                     ", .vertex_store_type = " +
+                     (c->vertex_store_type ? "Bitmap" : "Array") +
+                     "}, .infra_config = {.graph_backend_type = InMemory}, "
+                     ".engine_config = {.launch_config = {.num_blocks = " +
+                     std::to_string(c->num_blocks) + ", .threads_per_block = " +
+                     std::to_string(c->threads_per_block) +
+                     ", .threads_per_warp = " + std::to_string(c->threads_per_warp) +
+                     ", .max_regs = " + std::to_string(c->max_regs) + "}}}";
+    return copy_out(s, buf, cap, nullptr);
+}
+
+// -------------------------------------------------------------- graph
+
+int gat_graph_load(const char *path, int binary, gat_graph **out) {
+    if (!path || !out) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    auto g = std::make_unique<gat_graph>();
+    std::string err;
+    bool ok = binary ? load_binary(path, g->host, &err) : load_text(path, g->host, &err);
+    if (!ok) return fail(GAT_ERR_IO, err);
+    if (!validate(g->host, false, &err)) return fail(GAT_ERR_IO, "invalid CSR: " + err);
+    *out = g.release();
+    return GAT_OK;
+}
+
+int gat_graph_from_csr(int32_t V, int64_t E, const int64_t *offsets,
+                       const int32_t *adj, gat_graph **out) {
+    if (!out || V < 0 || E < 0 || !offsets || (E > 0 && !adj))
+        return fail(GAT_ERR_ARGUMENT, "bad CSR arguments");
+    *out = nullptr;
+    auto g = std::make_unique<gat_graph>();
+    g->host.V = V;
+    g->host.E = E;
+    g->host.off.assign(offsets, offsets + V + 1);
+    g->host.adj.assign(adj, adj + E);
+    std::string err;
+    if (!validate(g->host, true, &err)) return fail(GAT_ERR_ARGUMENT, "invalid CSR: " + err);
+    *out = g.release();
+    return GAT_OK;
+}
+
+int gat_graph_generate(int kind, double p0, double p1, double p2, double p3,
+                       double p4, uint64_t seed, gat_graph **out) {
+    if (!out) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    auto g = std::make_unique<gat_graph>();
+    if (kind == 0) {
+        if (p0 < 0 || p0 > INT32_MAX || p1 < 0) return fail(GAT_ERR_ARGUMENT, "bad ER parameters");
+        gen_erdos_renyi((int32_t)p0, p1, seed, g->host);
+    } else if (kind == 1) {
+        if (p0 < 1 || p0 > 30 || p1 < 0 || p2 < 0 || p3 < 0 || p4 < 0 || p2 + p3 + p4 > 1)
+            return fail(GAT_ERR_ARGUMENT, "bad R-MAT parameters");
+        gen_rmat((int)p0, (int64_t)p1, p2, p3, p4, seed, g->host);
+    } else if (kind == 2) {
+        if (p0 < 0 || p0 > INT32_MAX || p1 < 1) return fail(GAT_ERR_ARGUMENT, "bad BA parameters");
+        gen_barabasi_albert((int32_t)p0, (int32_t)p1, seed, g->host);
+    } else {
+        return fail(GAT_ERR_ARGUMENT, "unknown generator");
+    }
+    *out = g.release();
+    return GAT_OK;
+}
+
+int gat_graph_save(const gat_graph *g, const char *path) {
+    if (!g || !path) return fail(GAT_ERR_ARGUMENT, "null argument");
+    std::string err;
+    if (!save_binary(path, g->host, &err)) return fail(GAT_ERR_IO, err);
+    return GAT_OK;
+}
+
+int gat_graph_info(const gat_graph *g, int32_t *V, int64_t *E, int32_t *max_degree) {
+    if (!g) return fail(GAT_ERR_ARGUMENT, "null argument");
+    if (V) *V = g->host.V;
+    if (E) *E = g->host.E;
+    if (max_degree) *max_degree = g->host.max_degree();
+    return GAT_OK;
+}
+
+int gat_graph_csr(const gat_graph *g, const int64_t **offsets, const int32_t **adj) {
+    if (!g || !offsets || !adj) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *offsets = g->host.off.data();
+    *adj = g->host.adj.data();
+    return GAT_OK;
+}
+
+namespace {
+int upload_copy(const HostGraph &h, DevCopy &d, cudaStream_t st) {
+    d.release();
+    std::vector<int64_t> lo(size_t(h.V) + 1, 0);
+    for (int32_t v = 0; v < h.V; v++) {
+        auto b = h.adj.begin() + h.off[v], e = h.adj.begin() + h.off[v + 1];
+        lo[v + 1] = lo[v] + (std::lower_bound(b, e, v) - b);
+    }
+    cudaError_t e;
+    if ((e = cudaMalloc(&d.off, sizeof(int64_t) * (h.V + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&d.adj, sizeof(int32_t) * std::max<int64_t>(h.E, 1))) != cudaSuccess ||
+        (e = cudaMalloc(&d.lo_off, sizeof(int64_t) * (h.V + 1))) != cudaSuccess) {
+        d.release();
+        return fail(GAT_ERR_MEMORY, std::string("device graph allocation: ") + cudaGetErrorString(e));
+    }
+    if ((e = cudaMemcpyAsync(d.off, h.off.data(), sizeof(int64_t) * (h.V + 1),
+                             cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (h.E > 0 && (e = cudaMemcpyAsync(d.adj, h.adj.data(), sizeof(int32_t) * h.E,
+                                         cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+        (e = cudaMemcpyAsync(d.lo_off, lo.data(), sizeof(int64_t) * (h.V + 1),
+                             cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        d.release();
+        return cuda_fail(e, "graph upload");
+    }
+    d.lo_total = lo[h.V];
+    d.max_degree = h.max_degree();
+    d.ready = true;
+    return GAT_OK;
+}
+}  // namespace
+
+int gat_graph_upload(gat_graph *g, int flags, void *stream) {
+    if (!g) return fail(GAT_ERR_ARGUMENT, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    int rc = upload_copy(g->host, g->dev, st);
+    if (rc != GAT_OK) return rc;
+    if (flags & GAT_UPLOAD_DEGREE_ORDER) {
+        HostGraph r;
+        relabel_by_degree(g->host, r, nullptr);
+        rc = upload_copy(r, g->dev_ordered, st);
+        if (rc != GAT_OK) return rc;
+    } else {
+        g->dev_ordered.release();
+    }
+    g->device = dev;
+    return GAT_OK;
+}
+
+void gat_graph_free(gat_graph *g) { delete g; }
+
+// ------------------------------------------------------------- engine
+
+int gat_executor_create(const gat_config *c, gat_executor **out) {
+    if (!out) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    auto e = std::make_unique<gat_executor>();
+    if (c)
+        e->cfg = *c;
+    else
+        gat_config_engine_default(&e->cfg);
+    const gat_config &k = e->cfg;
+    int t = k.set_intersection_type == 1 ? 1 : k.threads_per_warp;
+    if (t != 1 && t != 2 && t != 4 && t != 8 && t != 16 && t != 32)
+        return fail(GAT_ERR_CONFIG, "threads_per_warp must be 1, 2, 4, 8, 16 or 32");
+    if (k.threads_per_block < 32 || k.threads_per_block > 256 ||
+        k.threads_per_block % 32 != 0)
+        return fail(GAT_ERR_CONFIG, "threads_per_block must be a multiple of 32 in [32, 256]");
+    if (k.num_blocks < 0) return fail(GAT_ERR_CONFIG, "num_blocks must be >= 0");
+    if (k.vertex_store_type != 0 || k.graph_backend_type != 0)
+        return fail(GAT_ERR_CONFIG, "only Array vertex sets and the InMemory backend exist");
+    cudaError_t ce;
+    if ((ce = cudaGetDevice(&e->device)) != cudaSuccess) return cuda_fail(ce, "cudaGetDevice");
+    if ((ce = cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->device)) !=
+        cudaSuccess)
+        return cuda_fail(ce, "device attributes");
+    if ((ce = cudaMalloc(&e->ctr, sizeof(DevCounters))) != cudaSuccess ||
+        (ce = cudaMalloc(&e->d_plan, sizeof(GatPlan))) != cudaSuccess ||
+        (ce = cudaMallocHost(&e->host_ctr, sizeof(DevCounters))) != cudaSuccess ||
+        (ce = cudaMallocHost(&e->h_plan, sizeof(GatPlan))) != cudaSuccess ||
+        (ce = cudaEventCreate(&e->ev0)) != cudaSuccess ||
+        (ce = cudaEventCreate(&e->ev1)) != cudaSuccess)
+        return cuda_fail(ce, "executor allocation");
+    *out = e.release();
+    return GAT_OK;
+}
+
+void gat_executor_free(gat_executor *e) { delete e; }
+
+namespace {
+
+int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *stream,
+               uint64_t *count, gat_stats *stats, bool balg) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!e || !g || !s || !count) return fail(GAT_ERR_ARGUMENT, "null argument");
+    gat_stats st{};
+    cudaStream_t strm = (cudaStream_t)stream;
+    if (s->trivial) {
+        int64_t c = 0;
+        if (s->mode == GAT_MODE_EXACT)
+            c = s->pattern.n == 1 ? g->host.V : g->host.E / 2;
+        *count = (uint64_t)c;
+        st.raw_sum = c;
+        st.divisor = 1;
+        if (stats) *stats = st;
+        return GAT_OK;
+    }
+    const GatPlan &plan = s->plan.plan;
+    if (plan.n == 0) return fail(GAT_ERR_UNDEFINED, s->plan.summary);
+    DevCopy *dc = nullptr;
+    if (s->mode == GAT_MODE_EXACT) {
+        if (!g->dev.ready) {
+            int rc = gat_graph_upload(g, GAT_UPLOAD_DEGREE_ORDER, stream);
+            if (rc != GAT_OK) return rc;
+        }
+        dc = g->dev_ordered.ready ? &g->dev_ordered : &g->dev;
+    } else {
+        if (!g->dev.ready) {
+            int rc = gat_graph_upload(g, 0, stream);
+            if (rc != GAT_OK) return rc;
+        }
+        dc = &g->dev;
+    }
+    DevGraphView view;
+    view.V = g->host.V;
+    view.E = g->host.E;
+    view.off = dc->off;
+    view.adj = dc->adj;
+    view.lo_off = dc->lo_off;
+    view.lo_total = dc->lo_total;
+    view.max_degree = dc->max_degree;
+
+    LaunchShape shape;
+    shape.tile = e->cfg.set_intersection_type == 1 ? 1 : e->cfg.threads_per_warp;
+    shape.block = e->cfg.threads_per_block;
+    shape.chunk = e->cfg.chunk > 0 ? e->cfg.chunk : 16;
+    shape.linear_below = e->cfg.set_search_type;
+    int occ = blocks_per_sm(shape.tile, shape.block, balg);
+    if (occ <= 0) return fail(GAT_ERR_CUDA, "kernel does not fit on the device");
+    shape.grid = e->cfg.num_blocks > 0 ? e->cfg.num_blocks : e->sms * occ;
+    const int64_t stride = tile_scratch_ints(plan, view.max_degree);
+    const int64_t tiles_per_block = shape.block / shape.tile;
+    const int64_t budget = e->cfg.memory_budget > 0 ? e->cfg.memory_budget : (int64_t(4) << 30);
+    int64_t per_block = tiles_per_block * stride * (int64_t)sizeof(int32_t);
+    if (plan.num_store > 0) {
+        int64_t max_grid = budget / per_block;
+        if (max_grid < 1)
+            return fail(GAT_ERR_MEMORY, "memory budget below one CTA's scratch");
+        if (shape.grid > max_grid) shape.grid = (int)max_grid;
+    }
+    size_t need = (size_t)(plan.num_store > 0 ? per_block * shape.grid : 4);
+    cudaError_t ce;
+    if (need > e->scratch_bytes) {
+        cudaFree(e->scratch);
+        e->scratch = nullptr;
+        e->scratch_bytes = 0;
+        if ((ce = cudaMalloc(&e->scratch, need)) != cudaSuccess)
+            return fail(GAT_ERR_MEMORY, std::string("scratch allocation: ") + cudaGetErrorString(ce));
+        e->scratch_bytes = need;
+    }
+    *e->h_plan = plan;
+    if ((ce = cudaMemcpyAsync(e->d_plan, e->h_plan, sizeof(GatPlan), cudaMemcpyHostToDevice,
+                              strm)) != cudaSuccess)
+        return cuda_fail(ce, "plan upload");
+    cudaEventRecord(e->ev0, strm);
+    ce = launch_search(e->d_plan, plan, view, shape, e->scratch, stride, e->ctr, balg, strm);
+    if (ce != cudaSuccess) return cuda_fail(ce, "search launch");
+    cudaEventRecord(e->ev1, strm);
+    if ((ce = cudaMemcpyAsync(e->host_ctr, e->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                              strm)) != cudaSuccess ||
+        (ce = cudaStreamSynchronize(strm)) != cudaSuccess)
+        return cuda_fail(ce, "search");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    if (e->host_ctr->error) return fail(GAT_ERR_DEVICE, "kernel reported an internal error");
+    int64_t raw = (int64_t)e->host_ctr->result;
+    if (plan.divisor <= 0 || raw % plan.divisor != 0)
+        return fail(GAT_ERR_DEVICE, "engine total is not a multiple of the plan divisor");
+    *count = (uint64_t)(raw / plan.divisor);
+    st.kernel_ms = ms;
+    st.raw_sum = raw;
+    st.divisor = plan.divisor;
+    st.tasks = plan.level1_bounded ? (uint64_t)view.lo_total : (uint64_t)view.E;
+    st.balg_bytes = e->host_ctr->bytes;
+    st.grid = shape.grid;
+    st.block = shape.block;
+    st.tile = shape.tile;
+    st.launches = 1;
+    st.scratch_bytes = plan.num_store > 0 ? per_block * shape.grid : 0;
+    st.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                      .count();
+    if (stats) *stats = st;
+    return GAT_OK;
+}
+
+}  // namespace
+
+int gat_executor_count(gat_executor *e, gat_graph *g, const gat_schedule *s, void *stream,
+                       uint64_t *count, gat_stats *stats) {
+    return count_impl(e, g, s, stream, count, stats, false);
+}
+
+int gat_executor_count_balg(gat_executor *e, gat_graph *g, const gat_schedule *s,
+                            void *stream, uint64_t *count, gat_stats *stats) {
+    return count_impl(e, g, s, stream, count, stats, true);
+}
+
+int gat_count(gat_graph *g, const gat_schedule *s, const gat_config *c, uint64_t *count,
+              gat_stats *stats) {
+    gat_executor *e = nullptr;
+    int rc = gat_executor_create(c, &e);
+    if (rc != GAT_OK) return rc;
+    rc = gat_executor_count(e, g, s, nullptr, count, stats);
+    gat_executor_free(e);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,499 @@
+// The pattern-counting search kernel for sm_100a.
+//
+// Work decomposition.  The reference expands whole BFS levels from the host
+// (engine/engine.cuh:232-319): one prepare kernel, a cub scan, a device->host
+// copy and a stream sync per (level, chunk), storing max-degree ints per unit
+// per prefix.  Here one persistent launch does the whole search:
+//
+//  * The level-1 units (v0, v1) are the work queue.  They are numbered by
+//    CSR entry (or, when the plan bounds v1 < v0, by entry among each row's
+//    lower neighbours) and handed out in chunks through one atomic cursor,
+//    which balances power-law rows across the grid.
+//  * A tile of G lanes (G = the reference's threads_per_warp knob) owns one
+//    unit at a time and walks levels 2 .. basic-1 depth-first; its state
+//    (embedding, per-level candidate cursor, per-prefix set descriptor) lives
+//    in shared memory.  Sets that later levels intersect with are written to
+//    a per-tile scratch slot of max-degree ints; only one chain of sets per
+//    tile is live, so scratch is tiles x slots x max_degree, not
+//    units x prefixes x max_degree.
+//  * Set intersection is tile-cooperative: each lane takes elements of the
+//    shorter sorted list and searches the longer one (branch-free binary
+//    search, or a linear scan below the set_search_type threshold); stored
+//    outputs are compacted in order with ballot + popc.  Bounds from the
+//    symmetry-breaking conditions truncate both inputs first (lower_bound,
+//    G-ary when G >= 8).
+//  * At the last enumerated level the inclusion-exclusion value of the unit
+//    is formed from the IEP set sizes and added to a per-tile int64
+//    accumulator; each tile adds it to the global total once at exit.
+//
+// The kernel has no waits on other CTAs: the only inter-CTA interaction is
+// atomicAdd on the cursor and the totals.
+#include <climits>
+#include <cstdio>
+
+#include "engine.hpp"
+
+namespace gat {
+namespace {
+
+constexpr int32_t kInf = INT32_MAX;
+
+struct TileSmem {
+    int32_t v[GAT_MAX_VERTICES];
+    int32_t cnt[GAT_MAX_VERTICES];
+    int32_t pos[GAT_MAX_VERTICES];
+    int32_t sl[GAT_MAX_PREFIX];
+    int32_t pad[2];
+    const int32_t *src[GAT_MAX_VERTICES];
+    const int32_t *sp[GAT_MAX_PREFIX];
+    long long val[GAT_MAX_PREFIX];
+};
+
+struct SearchArgs {
+    const GatPlan *plan;
+    const int64_t *off;
+    const int32_t *adj;
+    const int64_t *lo_off;
+    int32_t V;
+    int32_t cap;
+    int64_t num_tasks;
+    DevCounters *ctr;
+    int32_t *scratch;
+    int64_t scratch_stride;
+    int32_t chunk;
+    int32_t linear_below;
+};
+
+template <int G>
+struct Tile {
+    unsigned mask;
+    int lane;
+    int base;
+    __device__ __forceinline__ Tile() {
+        const int wl = threadIdx.x & 31;
+        lane = wl & (G - 1);
+        base = wl - lane;
+        mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << base);
+    }
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+    __device__ __forceinline__ unsigned ballot(bool p) const {
+        const unsigned b = __ballot_sync(mask, p);
+        return G == 32 ? b : ((b >> base) & ((1u << G) - 1u));
+    }
+    template <class T>
+    __device__ __forceinline__ T bcast(T x, int src) const {
+        return __shfl_sync(mask, x, src, G);
+    }
+    template <class T>
+    __device__ __forceinline__ T sum(T x) const {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) x += __shfl_xor_sync(mask, x, o, G);
+        return x;
+    }
+};
+
+__device__ __forceinline__ int32_t min_of(const TileSmem &S, unsigned m) {
+    int32_t r = kInf;
+    while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1;
+        r = min(r, S.v[j]);
+    }
+    return r;
+}
+
+// First index i in a[0, n) with a[i] >= x (lower) or a[i] > x (upper),
+// computed identically on every lane of the tile.
+template <int G, bool UPPER, class T>
+__device__ __forceinline__ int tile_bound(const Tile<G> &t, const T *a, int n,
+                                          T x) {
+    if (G < 8) {
+        int lo = 0, len = n;
+        while (len > 0) {
+            const int h = len >> 1;
+            const T y = a[lo + h];
+            const bool go = UPPER ? (y <= x) : (y < x);
+            if (go) {
+                lo += h + 1;
+                len -= h + 1;
+            } else {
+                len = h;
+            }
+        }
+        return lo;
+    }
+    int lo = 0, hi = n;
+    while (hi - lo > G) {
+        const int p = lo + (int)(((long long)(t.lane + 1) * (hi - lo)) / (G + 1));
+        const T y = a[p];
+        const bool less = UPPER ? (y <= x) : (y < x);
+        const int c = __popc(t.ballot(less));
+        const int plo = t.bcast(p, c > 0 ? c - 1 : 0);
+        const int phi = t.bcast(p, c < G ? c : G - 1);
+        const int nlo = c > 0 ? plo + 1 : lo;
+        const int nhi = c < G ? phi : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    bool less = false;
+    if (lo + t.lane < hi) {
+        const T y = a[lo + t.lane];
+        less = UPPER ? (y <= x) : (y < x);
+    }
+    return lo + __popc(t.ballot(less));
+}
+
+// Membership of x in the sorted list b[0, nb): branch-free binary search
+// (largest element <= x), or a linear scan for short lists.
+__device__ __forceinline__ bool contains(const int32_t *b, int nb, int32_t x,
+                                         int linear_below) {
+    if (nb <= 0) return false;
+    if (nb < linear_below) {
+        for (int i = 0; i < nb; i++) {
+            const int32_t y = b[i];
+            if (y >= x) return y == x;
+        }
+        return false;
+    }
+    int lo = 0, len = nb;
+    while (len > 1) {
+        const int h = len >> 1;
+        lo = (b[lo + h] <= x) ? lo + h : lo;
+        len -= h;
+    }
+    return b[lo] == x;
+}
+
+template <int G>
+__device__ __forceinline__ int isect_count(const Tile<G> &t, const int32_t *a,
+                                           int na, const int32_t *b, int nb,
+                                           const TileSmem &S, unsigned excl,
+                                           int linear_below) {
+    if (na > nb) {
+        const int32_t *tp = a;
+        a = b;
+        b = tp;
+        const int tn = na;
+        na = nb;
+        nb = tn;
+    }
+    int c = 0;
+    for (int i = t.lane; i < na; i += G) {
+        const int32_t x = a[i];
+        bool ok = contains(b, nb, x, linear_below);
+        unsigned m = excl;
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            ok &= (S.v[j] != x);
+        }
+        c += ok ? 1 : 0;
+    }
+    return t.sum(c);
+}
+
+template <int G>
+__device__ __forceinline__ int isect_store(const Tile<G> &t, const int32_t *a,
+                                           int na, const int32_t *b, int nb,
+                                           int32_t *out, int linear_below) {
+    if (na > nb) {
+        const int32_t *tp = a;
+        a = b;
+        b = tp;
+        const int tn = na;
+        na = nb;
+        nb = tn;
+    }
+    int n = 0;
+    for (int base = 0; base < na; base += G) {
+        const int i = base + t.lane;
+        bool f = false;
+        int32_t x = 0;
+        if (i < na) {
+            x = a[i];
+            f = contains(b, nb, x, linear_below);
+        }
+        const unsigned m = t.ballot(f);
+        if (f) out[n + __popc(m & ((1u << t.lane) - 1u))] = x;
+        n += __popc(m);
+    }
+    return n;
+}
+
+// Builds every prefix set that ends at level k for candidate v.
+template <int G, bool STATS>
+__device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
+                           const SearchArgs &a, int k, int32_t v, bool collided,
+                           int32_t *scratch, unsigned long long &bytes) {
+    const int64_t o = a.off[v];
+    const int32_t *nb = a.adj + o;
+    const int32_t dv = (int32_t)(a.off[v + 1] - o);
+    const int pe = P.l_pbegin[k + 1];
+    for (int p = P.l_pbegin[k]; p < pe; p++) {
+        const int kind = P.p_kind[p];
+        const int32_t *ptr = S.sp[p];
+        int32_t len = 0;
+        if (!collided) {
+            const int32_t T = min_of(S, P.p_trunc[p]);
+            if (kind == GAT_SET_ALIAS) {
+                ptr = nb;
+                len = (T == kInf) ? dv : tile_bound<G, false>(t, nb, dv, T);
+            } else {
+                const int f = P.p_father[p];
+                const int32_t *fp = S.sp[f];
+                int32_t fl = S.sl[f];
+                int32_t nl = dv;
+                if (T != kInf) {
+                    fl = tile_bound<G, false>(t, fp, fl, T);
+                    nl = tile_bound<G, false>(t, nb, dv, T);
+                }
+                if (STATS && t.lane == 0) bytes += 4ull * (unsigned)(nl + fl);
+                if (kind == GAT_SET_STORE) {
+                    int32_t *out = scratch + (int64_t)P.p_slot[p] * a.cap;
+                    len = isect_store(t, nb, nl, fp, fl, out, a.linear_below);
+                    ptr = out;
+                    if (STATS && t.lane == 0) bytes += 4ull * (unsigned)len;
+                } else {
+                    len = isect_count(t, nb, nl, fp, fl, S, P.p_excl[p],
+                                      a.linear_below);
+                }
+            }
+        }
+        if (t.lane == 0) {
+            S.sp[p] = ptr;
+            S.sl[p] = len;
+        }
+        t.sync();
+    }
+}
+
+template <int G>
+__device__ __forceinline__ void setup_level(const Tile<G> &t, TileSmem &S,
+                                            const GatPlan &P, int k) {
+    const int lp = P.l_loop[k];
+    const int32_t *ptr = S.sp[lp];
+    const int32_t len = S.sl[lp];
+    const int32_t B = min_of(S, P.l_bound[k]);
+    const int32_t cnt = (B == kInf) ? len : tile_bound<G, false>(t, ptr, len, B);
+    if (t.lane == 0) {
+        S.src[k] = ptr;
+        S.cnt[k] = cnt;
+        S.pos[k] = 0;
+    }
+    t.sync();
+}
+
+// Inclusion-exclusion value of the current unit (valid on lane 0).
+template <int G>
+__device__ long long iep_value(const Tile<G> &t, TileSmem &S, const GatPlan &P,
+                               int linear_below) {
+    const int basic = P.basic;
+    for (int x = 0; x < P.iep_num; x++) {
+        const int p = P.iep_prefix[x];
+        long long val;
+        if (P.p_kind[p] == GAT_SET_COUNT) {
+            val = S.sl[p];
+        } else {
+            const int32_t *ptr = S.sp[p];
+            int32_t len = S.sl[p];
+            const int32_t B = min_of(S, P.iep_bound[x]);
+            if (B != kInf) len = tile_bound<G, false>(t, ptr, len, B);
+            const unsigned m = P.iep_sub[x];
+            int hit = 0;
+            for (int j = t.lane; j < basic; j += G)
+                if ((m >> j) & 1u) hit += contains(ptr, len, S.v[j], linear_below);
+            hit = t.sum(hit);
+            val = (long long)len - hit;
+        }
+        if (t.lane == 0) S.val[x] = val;
+    }
+    unsigned long long local = 0, cur = 1;
+    if (t.lane == 0) {
+        int last = -1;
+        for (int g = 0; g < P.num_terms; g++) {
+            const unsigned long long v = (unsigned long long)S.val[P.t_slot[g]];
+            cur = (g == last + 1) ? v : cur * v;
+            if (P.t_close[g]) {
+                last = g;
+                local += cur * (unsigned long long)(long long)P.t_coef[g];
+            }
+        }
+    }
+    return (long long)local;
+}
+
+template <int G, bool STATS>
+__global__ void __launch_bounds__(256)
+    search_kernel(const SearchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Tile<G> t;
+    const int tiles_per_block = blockDim.x / G;
+    const int tile_in_block = threadIdx.x / G;
+    TileSmem &S = reinterpret_cast<TileSmem *>(smem_raw)[tile_in_block];
+    const GatPlan &P = *a.plan;
+    const int basic = P.basic;
+    int32_t *scratch =
+        a.scratch + ((int64_t)blockIdx.x * tiles_per_block + tile_in_block) *
+                        a.scratch_stride;
+    const int64_t *task_off = P.level1_bounded ? a.lo_off : a.off;
+    unsigned long long acc = 0, bytes = 0;
+
+    for (;;) {
+        unsigned long long start = 0;
+        if (t.lane == 0) start = atomicAdd(&a.ctr->cursor, (unsigned long long)a.chunk);
+        start = t.bcast(start, 0);
+        if (start >= (unsigned long long)a.num_tasks) break;
+        const int64_t end = min((int64_t)start + a.chunk, a.num_tasks);
+        int32_t row =
+            tile_bound<G, true, int64_t>(t, task_off, a.V + 1, (int64_t)start) - 1;
+        int32_t cur_v0 = -1;
+        for (int64_t tk = (int64_t)start; tk < end; tk++) {
+            while (task_off[row + 1] <= tk) row++;
+            const int32_t v0 = row;
+            const int32_t v1 = a.adj[a.off[v0] + (tk - task_off[v0])];
+            if (v0 != cur_v0) {
+                if (t.lane == 0) S.v[0] = v0;
+                t.sync();
+                level_sets<G, STATS>(t, S, P, a, 0, v0, false, scratch, bytes);
+                cur_v0 = v0;
+            }
+            if (t.lane == 0) S.v[1] = v1;
+            t.sync();
+            level_sets<G, STATS>(t, S, P, a, 1, v1, false, scratch, bytes);
+            if (basic == 2) {
+                const long long r = iep_value(t, S, P, a.linear_below);
+                if (t.lane == 0) acc += (unsigned long long)r;
+                t.sync();
+                continue;
+            }
+            setup_level(t, S, P, 2);
+            int k = 2;
+            while (k >= 2) {
+                if (S.pos[k] >= S.cnt[k]) {
+                    k--;
+                    continue;
+                }
+                const int32_t cand = S.src[k][S.pos[k]];
+                bool hit = false;
+                unsigned dm = P.l_distinct[k];
+                while (dm) {
+                    const int j = __ffs(dm) - 1;
+                    dm &= dm - 1;
+                    hit |= (S.v[j] == cand);
+                }
+                t.sync();
+                if (t.lane == 0) S.pos[k]++;
+                if (hit && !P.collide_clear) {
+                    t.sync();
+                    continue;
+                }
+                if (t.lane == 0) S.v[k] = cand;
+                t.sync();
+                level_sets<G, STATS>(t, S, P, a, k, cand, hit, scratch, bytes);
+                if (k == basic - 1) {
+                    const long long r = iep_value(t, S, P, a.linear_below);
+                    if (t.lane == 0) acc += (unsigned long long)r;
+                    t.sync();
+                    continue;
+                }
+                setup_level(t, S, P, k + 1);
+                k++;
+            }
+        }
+    }
+    if (t.lane == 0) {
+        atomicAdd(&a.ctr->result, acc);
+        if (STATS) atomicAdd(&a.ctr->bytes, bytes);
+    }
+}
+
+template <int G, bool STATS>
+cudaError_t launch_one(const SearchArgs &a, int grid, int block,
+                       cudaStream_t stream) {
+    const size_t smem = size_t(block / G) * sizeof(TileSmem);
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaError_t e = cudaFuncSetAttribute(
+            search_kernel<G, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            227 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_done = true;
+    }
+    search_kernel<G, STATS><<<grid, block, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+template <bool STATS>
+cudaError_t dispatch(const SearchArgs &a, int tile, int grid, int block,
+                     cudaStream_t s) {
+    switch (tile) {
+        case 1: return launch_one<1, STATS>(a, grid, block, s);
+        case 2: return launch_one<2, STATS>(a, grid, block, s);
+        case 4: return launch_one<4, STATS>(a, grid, block, s);
+        case 8: return launch_one<8, STATS>(a, grid, block, s);
+        case 16: return launch_one<16, STATS>(a, grid, block, s);
+        case 32: return launch_one<32, STATS>(a, grid, block, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int G, bool STATS>
+int occupancy(int block) {
+    int n = 0;
+    const size_t smem = size_t(block / G) * sizeof(TileSmem);
+    cudaFuncSetAttribute(search_kernel<G, STATS>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, search_kernel<G, STATS>, block, smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+}  // namespace
+
+size_t tile_smem_bytes() { return sizeof(TileSmem); }
+
+int blocks_per_sm(int tile, int block, bool stats) {
+#define GAT_OCC(G) \
+    return stats ? occupancy<G, true>(block) : occupancy<G, false>(block)
+    switch (tile) {
+        case 1: GAT_OCC(1);
+        case 2: GAT_OCC(2);
+        case 4: GAT_OCC(4);
+        case 8: GAT_OCC(8);
+        case 16: GAT_OCC(16);
+        case 32: GAT_OCC(32);
+        default: return 0;
+    }
+#undef GAT_OCC
+}
+
+int64_t tile_scratch_ints(const GatPlan &plan, int32_t max_degree) {
+    return int64_t(plan.num_store) * int64_t(max_degree > 0 ? max_degree : 1);
+}
+
+cudaError_t launch_search(const GatPlan *d_plan, const GatPlan &h_plan,
+                          const DevGraphView &g, const LaunchShape &shape,
+                          int32_t *scratch, int64_t scratch_stride,
+                          DevCounters *counters, bool stats,
+                          cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(DevCounters), stream);
+    if (e != cudaSuccess) return e;
+    SearchArgs a;
+    a.plan = d_plan;
+    a.off = g.off;
+    a.adj = g.adj;
+    a.lo_off = g.lo_off;
+    a.V = g.V;
+    a.cap = g.max_degree > 0 ? g.max_degree : 1;
+    a.num_tasks = h_plan.level1_bounded ? g.lo_total : g.E;
+    a.ctr = counters;
+    a.scratch = scratch;
+    a.scratch_stride = scratch_stride;
+    a.chunk = shape.chunk > 0 ? shape.chunk : 1;
+    a.linear_below = shape.linear_below;
+    return stats ? dispatch<true>(a, shape.tile, shape.grid, shape.block, stream)
+                 : dispatch<false>(a, shape.tile, shape.grid, shape.block, stream);
+}
+
+}  // namespace gat

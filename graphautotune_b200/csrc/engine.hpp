@@ -1,0 +1,61 @@
+// Host-side interface of the CUDA search engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gat_plan.h"
+
+namespace gat {
+
+// A graph resident on the device.  `task_off` arrays index the level-1
+// units: lo_off[v] = number of entries u < v in rows before v (rows are
+// sorted, so a row's entries u < v are its prefix).
+struct DevGraphView {
+    int32_t V = 0;
+    int64_t E = 0;
+    const int64_t *off = nullptr;
+    const int32_t *adj = nullptr;
+    const int64_t *lo_off = nullptr;
+    int64_t lo_total = 0;  // lo_off[V]
+    int32_t max_degree = 0;
+};
+
+struct LaunchShape {
+    int grid = 0;         // CTAs
+    int block = 128;      // threads per CTA
+    int tile = 32;        // lanes cooperating on one unit
+    int chunk = 16;       // level-1 units taken per queue grab
+    int linear_below = 0; // lists shorter than this are scanned linearly
+};
+
+// Device counters used by one search: work-queue cursor, signed 64-bit
+// total (two's complement in an unsigned word), algorithmic bytes, error
+// flags.
+struct DevCounters {
+    unsigned long long cursor;
+    unsigned long long result;
+    unsigned long long bytes;
+    unsigned long long error;
+};
+
+enum : unsigned long long {
+    GAT_DEVERR_SCRATCH = 1ull,  // a stored set would overflow its slot
+};
+
+// Shared memory one tile needs.
+size_t tile_smem_bytes();
+// Largest CTA count per SM for this tile/block/stats combination.
+int blocks_per_sm(int tile, int block, bool stats);
+// Scratch ints one tile needs for `plan` on a graph with this max degree.
+int64_t tile_scratch_ints(const GatPlan &plan, int32_t max_degree);
+
+// Launches the search kernel.  `counters` must be zeroed before the launch
+// (done here with cudaMemsetAsync on `stream`).  Returns a cudaError_t.
+cudaError_t launch_search(const GatPlan *d_plan, const GatPlan &h_plan,
+                          const DevGraphView &g, const LaunchShape &shape,
+                          int32_t *scratch, int64_t scratch_stride,
+                          DevCounters *counters, bool stats,
+                          cudaStream_t stream);
+
+}  // namespace gat

@@ -1,0 +1,206 @@
+/* libgat: B200 subgraph-counting engine, C ABI.
+ *
+ * Drop-in boundary for GraphAutoTune's pattern-matching path.  Each entry
+ * point names the reference interface it replaces (paths inside the
+ * reference project).  Plain pointers, sizes and status codes only; no C++
+ * or CUDA types cross this boundary (CUDA streams are passed as void*).
+ *
+ * Error behaviour: the reference exits the process on CUDA errors
+ * (utils/cuda_utils.cuh:7-16 gpuErrchk) and throws on I/O errors
+ * (target/pm.cu:16,24).  Here every call returns a gat_status; the message
+ * of the last failure on the calling thread is available from
+ * gat_last_error().  No call exits the process.
+ *
+ * Threading: handles are not internally locked; use one host thread per
+ * executor.  Graph and schedule handles may be shared read-only.
+ */
+#ifndef GAT_H
+#define GAT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gat_status {
+    GAT_OK = 0,
+    GAT_ERR_ARGUMENT = 1,    /* null pointer, size out of range */
+    GAT_ERR_PATTERN = 2,     /* malformed, disconnected or too large pattern */
+    GAT_ERR_IO = 3,          /* file missing, truncated or malformed */
+    GAT_ERR_CUDA = 4,        /* a CUDA runtime call failed */
+    GAT_ERR_MEMORY = 5,      /* allocation failed or memory budget too small */
+    GAT_ERR_UNDEFINED = 6,   /* the reference engine's result is undefined for
+                                this schedule (reads uninitialised state) */
+    GAT_ERR_DEVICE = 7,      /* the kernel reported an internal error */
+    GAT_ERR_STATE = 8,       /* handle in the wrong state (e.g. not uploaded) */
+    GAT_ERR_CONFIG = 9       /* unparsable or out-of-range configuration */
+} gat_status;
+
+/* Count semantics. */
+typedef enum gat_mode {
+    GAT_MODE_EXACT = 0,      /* number of (non-induced) subgraphs isomorphic to
+                                the pattern = labelled embeddings / |Aut| */
+    GAT_MODE_REF_COMPAT = 1  /* the value Executor::perform_search returns for
+                                the reference's own schedule
+                                (engine/engine.cuh:232-265) */
+} gat_mode;
+
+typedef struct gat_pattern gat_pattern;
+typedef struct gat_schedule gat_schedule;
+typedef struct gat_graph gat_graph;
+typedef struct gat_executor gat_executor;
+
+const char *gat_last_error(void);
+const char *gat_version(void);
+
+/* ------------------------------------------------------------- pattern --
+ * Replaces Core::Pattern(const std::string&) (core/pattern.hpp:22-39):
+ * n*n characters '0'/'1', row-major, symmetrised from either triangle,
+ * 1 <= n <= 10 (MAX_VERTEXES, consts/general_consts.hpp:3). */
+int gat_pattern_from_adj(const char *adj, gat_pattern **out);
+int gat_pattern_vertices(const gat_pattern *p);
+/* |Aut(p)| (core/schedule.hpp:189-191). */
+int gat_pattern_automorphisms(const gat_pattern *p, int64_t *out);
+/* Writes the symmetrised n*n adjacency string (+ NUL) into buf. */
+int gat_pattern_adjacency(const gat_pattern *p, char *buf, size_t cap);
+void gat_pattern_free(gat_pattern *p);
+/* All connected n-vertex patterns (n <= 6) up to isomorphism, each as its
+ * lexicographically smallest adjacency string, sorted, concatenated with
+ * '\n'.  *needed receives the byte count including the final NUL. */
+int gat_enumerate_patterns(int n, char *buf, size_t cap, size_t *needed);
+
+/* ------------------------------------------------------------ schedule --
+ * Replaces Core::Schedule(const Pattern&) (core/schedule.hpp:864-958) and
+ * Core::ScheduleData (core/schedule.hpp:984-1022).
+ *   GAT_MODE_REF_COMPAT: the reference's own schedule (same vertex order,
+ *     restrictions, prefixes and IEP groups), executed with the reference
+ *     engine's counting rules.
+ *   GAT_MODE_EXACT: a schedule for the exact count; `stats_graph` (nullable)
+ *     supplies data-graph statistics for ranking candidate vertex orders in
+ *     place of the reference's fixed v=5000, e=1e6, tri=1e4
+ *     (core/schedule.hpp:909-910). */
+int gat_schedule_build(const gat_pattern *p, int mode,
+                       const gat_graph *stats_graph, gat_schedule **out);
+int gat_schedule_mode(const gat_schedule *s);
+/* JSON with the fields of Schedule::output() (core/schedule.hpp:752-784)
+ * plus the chosen permutation and restrictions.  *needed = bytes incl NUL. */
+int gat_schedule_dump(const gat_schedule *s, char *buf, size_t cap,
+                      size_t *needed);
+/* Copies the device plan (struct GatPlan, graphautotune_b200/csrc/gat_plan.h)
+ * into buf; *needed = sizeof(GatPlan). */
+int gat_schedule_plan(const gat_schedule *s, void *buf, size_t cap,
+                      size_t *needed);
+void gat_schedule_free(gat_schedule *s);
+
+/* -------------------------------------------------------------- config --
+ * Runtime form of the compile-time Config (configs/config.hpp:10-14,
+ * vertex_set_config.hpp:3-17, infra_config.hpp:3-5, engine_config.hpp:3-11).
+ * The first eight fields keep the reference's names and meaning; the rest
+ * are this engine's own knobs. */
+typedef struct gat_config {
+    int32_t set_search_type;       /* lists shorter than this are scanned
+                                      linearly; 0 = always binary,
+                                      INT32_MAX = always linear */
+    int32_t set_intersection_type; /* 0 Parallel (tile-cooperative),
+                                      1 Serial (one lane per unit) */
+    int32_t vertex_store_type;     /* 0 Array (1 Bitmap is not implemented
+                                      in the reference either) */
+    int32_t graph_backend_type;    /* 0 InMemory */
+    int32_t num_blocks;            /* CTAs; 0 = persistent grid sized from
+                                      occupancy (SMs x resident CTAs) */
+    int32_t threads_per_block;     /* 32..256 */
+    int32_t threads_per_warp;      /* lanes per unit: 1,2,4,8,16,32 */
+    int32_t max_regs;              /* accepted for compatibility; register
+                                      use is fixed when the library is built */
+    int32_t chunk;                 /* level-1 units per work-queue grab */
+    int32_t reserved0;
+    int64_t memory_budget;         /* bytes of scratch the executor may hold;
+                                      0 = 4 GiB */
+    int64_t reserved[4];
+} gat_config;
+
+/* Defaults: the reference's generated default_config.hpp
+ * (include/generated/default_config.hpp:5): set_search_type 64, Parallel,
+ * Array, InMemory, 256 blocks, 128 threads, 1 thread per warp, 32 regs. */
+void gat_config_default(gat_config *c);
+/* This engine's tuned starting point (persistent grid, 32-lane tiles). */
+void gat_config_engine_default(gat_config *c);
+/* Parses either the designated-initializer text the tuner writes into
+ * default_config.hpp (tuning/tuning/config/base.py:286-293, e.g.
+ * "{.vertex_set_config = {.set_search_type = 64, ...}, ...}") or the flat
+ * JSON value dict of config.json (tuning/tuning/role/driver.py:50-51, keys
+ * like "engine_config.launch_config.num_blocks").  Unmentioned fields keep
+ * their current values. */
+int gat_config_parse(const char *text, gat_config *c);
+/* Writes the designated-initializer form (the text the tuner would emit). */
+int gat_config_format(const gat_config *c, char *buf, size_t cap);
+
+/* --------------------------------------------------------------- graph --
+ * Replaces Infra::GlobalMemoryGraph (infra/graph_backend.cuh:15-170).
+ * Binary layout: int32 V, int64 E (directed entries), int64 offsets[V+1],
+ * int32 neighbours[E]; text layout: "V E" then E lines "u v". */
+int gat_graph_load(const char *path, int binary, gat_graph **out);
+/* Copies caller CSR arrays (must be sorted, deduplicated, symmetric, no
+ * self loops; checked). */
+int gat_graph_from_csr(int32_t V, int64_t E, const int64_t *offsets,
+                       const int32_t *adj, gat_graph **out);
+/* Seeded synthetic graphs (splitmix64 streams).  kind: 0 Erdos-Renyi
+ * (p0 = n, p1 = avg degree), 1 R-MAT (p0 = scale, p1 = edge samples,
+ * p2..p4 = a, b, c), 2 Barabasi-Albert (p0 = n, p1 = m). */
+int gat_graph_generate(int kind, double p0, double p1, double p2, double p3,
+                       double p4, uint64_t seed, gat_graph **out);
+int gat_graph_save(const gat_graph *g, const char *path);
+int gat_graph_info(const gat_graph *g, int32_t *V, int64_t *E,
+                   int32_t *max_degree);
+/* Host CSR view (valid until gat_graph_free). */
+int gat_graph_csr(const gat_graph *g, const int64_t **offsets,
+                  const int32_t **adj);
+/* Copies the graph to the current device (GlobalMemoryGraph::to_device,
+ * graph_backend.cuh:102-118; the device copy is owned and freed by the
+ * handle).  flags: GAT_UPLOAD_DEGREE_ORDER also builds a copy relabelled by
+ * decreasing degree, which exact-mode counts use (exact counts do not depend
+ * on vertex ids; reference-compatible counts always use the ids as given). */
+#define GAT_UPLOAD_DEGREE_ORDER 1
+int gat_graph_upload(gat_graph *g, int flags, void *stream);
+void gat_graph_free(gat_graph *g);
+
+/* -------------------------------------------------------------- engine --
+ * Replaces Engine::Executor<config>(set_size, device) and
+ * long long Executor::perform_search(DeviceContext&)
+ * (engine/engine.cuh:157-265). */
+typedef struct gat_stats {
+    double kernel_ms;        /* device time of the search launch(es) */
+    double total_ms;         /* host wall time of the call */
+    int64_t raw_sum;         /* signed engine total before the divisor */
+    int64_t divisor;         /* embeddings per subgraph left by the plan */
+    uint64_t tasks;          /* level-1 units in the work queue */
+    uint64_t balg_bytes;     /* algorithmic bytes (when collected) */
+    int32_t grid, block, tile, launches;
+    int64_t scratch_bytes;
+} gat_stats;
+
+int gat_executor_create(const gat_config *c, gat_executor **out);
+void gat_executor_free(gat_executor *e);
+/* Counts `s` in `g` (uploaded, or uploaded on demand).  For GAT_MODE_EXACT
+ * *count is the subgraph count; for GAT_MODE_REF_COMPAT it holds the
+ * reference's signed long long result (two's complement).  stream may be
+ * NULL (default stream).  The call returns after the count is on the host.
+ * stats may be NULL. */
+int gat_executor_count(gat_executor *e, gat_graph *g, const gat_schedule *s,
+                       void *stream, uint64_t *count, gat_stats *stats);
+/* As gat_executor_count, and also measures the algorithmic bytes of every
+ * set operation (4(|A|+|B|) per intersection + 4|C| per stored output) with
+ * an instrumented launch. */
+int gat_executor_count_balg(gat_executor *e, gat_graph *g,
+                            const gat_schedule *s, void *stream,
+                            uint64_t *count, gat_stats *stats);
+/* One-shot convenience: executor from config (NULL = engine default). */
+int gat_count(gat_graph *g, const gat_schedule *s, const gat_config *c,
+              uint64_t *count, gat_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,113 @@
+"""Test infrastructure only: ctypes wrapper of the CPU oracle (liboracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+import this module, and only as the checker.  The product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-C", str(HERE), "liboracle.so"], check=True,
+                   capture_output=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        l = C.CDLL(str(LIB))
+        i64p, i32p = C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+        l.oracle_naive_labelled.restype = C.c_uint64
+        l.oracle_naive_labelled.argtypes = [C.c_int32, i64p, i32p, C.c_char_p, C.c_int32,
+                                            C.c_int32, C.c_int]
+        l.oracle_backtrack_labelled.restype = C.c_uint64
+        l.oracle_backtrack_labelled.argtypes = l.oracle_naive_labelled.argtypes
+        l.oracle_automorphisms.restype = C.c_int64
+        l.oracle_automorphisms.argtypes = [C.c_char_p]
+        l.oracle_ref_engine.restype = C.c_int
+        l.oracle_ref_engine.argtypes = [C.c_int32, i64p, i32p, i32p, C.c_int32, C.c_int32,
+                                        C.c_int32, C.c_int, i64p, C.POINTER(C.c_uint64)]
+        l.oracle_intersect_size.restype = C.c_int32
+        l.oracle_intersect_size.argtypes = [i32p, C.c_int32, i32p, C.c_int32]
+        _lib = l
+    return _lib
+
+
+def _csr(off: np.ndarray, adj: np.ndarray):
+    off = np.ascontiguousarray(off, np.int64)
+    adj = np.ascontiguousarray(adj if len(adj) else np.zeros(1, np.int32), np.int32)
+    return (len(off) - 1, off, adj,
+            off.ctypes.data_as(C.POINTER(C.c_int64)),
+            adj.ctypes.data_as(C.POINTER(C.c_int32)))
+
+
+def naive_labelled(off, adj, pattern: str, roots=None, threads: int = 0) -> int:
+    V, o, a, po, pa = _csr(off, adj)
+    b, e = roots if roots else (0, V)
+    return lib().oracle_naive_labelled(V, po, pa, pattern.encode(), b, e, threads)
+
+
+def backtrack_labelled(off, adj, pattern: str, roots=None, threads: int = 0) -> int:
+    V, o, a, po, pa = _csr(off, adj)
+    b, e = roots if roots else (0, V)
+    return lib().oracle_backtrack_labelled(V, po, pa, pattern.encode(), b, e, threads)
+
+
+def automorphisms(pattern: str) -> int:
+    return lib().oracle_automorphisms(pattern.encode())
+
+
+def exact_count(off, adj, pattern: str, threads: int = 0) -> int:
+    lab = backtrack_labelled(off, adj, pattern, threads=threads)
+    aut = automorphisms(pattern)
+    assert lab % aut == 0
+    return lab // aut
+
+
+def encode_schedule(sd: dict) -> np.ndarray:
+    """Flat ScheduleData encoding (see oracle.h) from a schedule dump."""
+    basic = sd["basic_vertexes"]
+    pre = sd["prefixs"]
+    rest = [r[0] for r in sd["restrictions"]]
+    out = [basic, len(pre), len(rest), len(sd["iep_vertex_id"]), len(sd["iep_ans_pos"])]
+    for p in pre:
+        out += [len(p), *p]
+    out += sd["prefixs_father"] + sd["prefixs_size_only"]
+    out += sd["sd_vertex_prefix_start"] + sd["loop_set_prefix_id"]
+    out += sd["sd_restrictions_start"] + rest
+    out += sd["iep_vertex_id"] + sd["iep_ans_pos"] + sd["iep_coef"]
+    out += [int(x) for x in sd["iep_flag"]]
+    return np.array(out, np.int32)
+
+
+REF_UNDEFINED = (-2, -3)
+
+
+def ref_engine(off, adj, sd: dict, roots=None, threads: int = 0):
+    """(status, total, balg) of the reference engine semantics."""
+    V, o, a, po, pa = _csr(off, adj)
+    flat = encode_schedule(sd)
+    b, e = roots if roots else (0, V)
+    out = C.c_int64()
+    balg = C.c_uint64()
+    st = lib().oracle_ref_engine(V, po, pa, flat.ctypes.data_as(C.POINTER(C.c_int32)),
+                                 len(flat), b, e, threads, C.byref(out), C.byref(balg))
+    return st, out.value, balg.value
+
+
+def intersect_size(a, b) -> int:
+    a = np.ascontiguousarray(a, np.int32)
+    b = np.ascontiguousarray(b, np.int32)
+    return lib().oracle_intersect_size(a.ctypes.data_as(C.POINTER(C.c_int32)), len(a),
+                                       b.ctypes.data_as(C.POINTER(C.c_int32)), len(b))

@@ -1,0 +1,120 @@
+"""GPU parity: libgat counts through the C ABI against the oracle and the
+reference's own answers.
+
+  * exact mode == naive_pm Answer / |Aut| (reference binary, golden file)
+  * ref mode   == the reference engine's per-unit rules (oracle restatement),
+                  and GAT_ERR_UNDEFINED exactly where the reference reads
+                  uninitialised state or crashes
+  * every launch shape (tile width, search type, chunk) gives the same count
+"""
+import pytest
+
+from graphautotune_b200._lib import GAT_ERR_UNDEFINED, GatError
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = [
+    dict(threads_per_warp=32, threads_per_block=256, num_blocks=0, set_search_type=0, chunk=8),
+    dict(threads_per_warp=8, threads_per_block=128, num_blocks=0, set_search_type=0, chunk=3),
+    dict(threads_per_warp=4, threads_per_block=64, num_blocks=7, set_search_type=16, chunk=1),
+    # the reference's generated default_config.hpp
+    dict(threads_per_warp=1, threads_per_block=128, num_blocks=256, set_search_type=64, chunk=16),
+]
+
+
+def _executor(gat, **kw):
+    c = gat.Config.engine_default()
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return gat.Executor(c)
+
+
+@pytest.fixture(scope="module")
+def executors(gat):
+    return [_executor(gat, **c) for c in CONFIGS]
+
+
+def test_exact_matches_naive_matcher(gat, oracle, golden_naive, golden_graphs, executors):
+    checked = 0
+    for e in golden_naive:
+        g = golden_graphs[e["graph"]]
+        s = gat.Schedule(e["adj"], "exact")
+        aut = oracle.automorphisms(e["adj"])
+        assert e["naive_answer"] % aut == 0
+        want = e["naive_answer"] // aut
+        for ex in executors:
+            got = ex.count(g, s).count
+            assert got == want, (e["graph"], e["pattern"], got, want)
+        checked += 1
+    assert checked > 300
+
+
+def test_ref_mode_matches_reference_engine_rules(gat, oracle, golden_schedules, golden_naive,
+                                                  golden_graphs, executors):
+    checked = undefined = 0
+    seen = set()
+    for e in golden_naive:
+        key = (e["graph"], e["adj"])
+        if key in seen:
+            continue
+        seen.add(key)
+        sd = golden_schedules[e["adj"]]
+        g = golden_graphs[e["graph"]]
+        off, adj = g.csr()
+        if sd.get("crash"):
+            with pytest.raises(GatError) as ei:
+                executors[0].count(g, gat.Schedule(e["adj"], "ref"))
+            assert ei.value.status == GAT_ERR_UNDEFINED
+            undefined += 1
+            continue
+        st, want, _ = oracle.ref_engine(off, adj, sd)
+        s = gat.Schedule(e["adj"], "ref")
+        if st in oracle.REF_UNDEFINED:
+            with pytest.raises(GatError) as ei:
+                executors[0].count(g, s)
+            assert ei.value.status == GAT_ERR_UNDEFINED
+            undefined += 1
+            continue
+        assert st == 0
+        for ex in executors:
+            got = ex.count(g, s).count
+            assert got == want, (e["graph"], e["pattern"], got, want)
+        checked += 1
+    assert checked > 200 and undefined > 0
+
+
+MEDIUM = [
+    ("er", (2000, 10.0), 5),
+    ("rmat", (11, 16384), 6),
+    ("ba", (3000, 4), 7),
+]
+NAMED = ["011101110", "0111101111011110", "0101101001011010",
+         "0100110110010110110010100", "0111110111110111110111110"]
+
+
+def _graph(gat, kind, params, seed):
+    if kind == "er":
+        return gat.Graph.erdos_renyi(*params, seed)
+    if kind == "rmat":
+        return gat.Graph.rmat(params[0], params[1], 0.57, 0.19, 0.19, seed)
+    return gat.Graph.barabasi_albert(*params, seed)
+
+
+@pytest.mark.parametrize("kind,params,seed", MEDIUM)
+def test_medium_graphs_exact_and_ref(gat, oracle, golden_schedules, kind, params, seed,
+                                     executors):
+    g = _graph(gat, kind, params, seed)
+    off, adj = g.csr()
+    pats = NAMED + gat.enumerate_patterns(5)
+    for p in pats:
+        want = oracle.exact_count(off, adj, p)
+        s = gat.Schedule(p, "exact")
+        for ex in executors[:2]:
+            assert ex.count(g, s).count == want, (kind, p)
+        sd = golden_schedules.get(p)
+        if sd is None or sd.get("crash"):
+            continue
+        st, ref_want, _ = oracle.ref_engine(off, adj, sd)
+        if st != 0:
+            continue
+        assert executors[0].count(g, gat.Schedule(p, "ref")).count == ref_want, (kind, p)

@@ -283,6 +283,30 @@ class Executor(_Handle):
         return CountResult(cnt, st.kernel_ms, st.total_ms, st.raw_sum, st.divisor, st.tasks,
                            st.balg_bytes, st.grid, st.block, st.tile, st.scratch_bytes)
 
+    def count_range(self, graph: Graph, schedule: Schedule, root_begin: int, root_end: int,
+                    stream: int | None = None) -> tuple[int, CountResult]:
+        """Undivided signed total over first vertices in [root_begin, root_end)."""
+        raw = C.c_int64()
+        st = gat_stats()
+        check(lib().gat_executor_count_range(self._h, graph._h, schedule._h,
+                                             C.c_void_p(stream) if stream else None,
+                                             root_begin, root_end, C.byref(raw), C.byref(st)))
+        return raw.value, CountResult(raw.value, st.kernel_ms, st.total_ms, st.raw_sum,
+                                      st.divisor, st.tasks, st.balg_bytes, st.grid, st.block,
+                                      st.tile, st.scratch_bytes)
+
+    def count_shard(self, graph: Graph, schedule: Schedule, shard: int, num_shards: int,
+                    stream: int | None = None) -> tuple[int, CountResult]:
+        """Undivided signed total of one equal slice of the work queue."""
+        raw = C.c_int64()
+        st = gat_stats()
+        check(lib().gat_executor_count_shard(self._h, graph._h, schedule._h,
+                                             C.c_void_p(stream) if stream else None,
+                                             shard, num_shards, C.byref(raw), C.byref(st)))
+        return raw.value, CountResult(raw.value, st.kernel_ms, st.total_ms, st.raw_sum,
+                                      st.divisor, st.tasks, st.balg_bytes, st.grid, st.block,
+                                      st.tile, st.scratch_bytes)
+
     def perform_search(self, graph: Graph, schedule: Schedule) -> int:
         """long long Executor::perform_search(DeviceContext&)."""
         return self.count(graph, schedule).count

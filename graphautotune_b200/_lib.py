@@ -104,6 +104,10 @@ _SIGS = {
     "gat_executor_count": (C.c_int, [P, P, P, P, C.POINTER(C.c_uint64), C.POINTER(gat_stats)]),
     "gat_executor_count_balg": (C.c_int, [P, P, P, P, C.POINTER(C.c_uint64),
                                           C.POINTER(gat_stats)]),
+    "gat_executor_count_range": (C.c_int, [P, P, P, P, C.c_int32, C.c_int32,
+                                           C.POINTER(C.c_int64), C.POINTER(gat_stats)]),
+    "gat_executor_count_shard": (C.c_int, [P, P, P, P, C.c_int32, C.c_int32,
+                                           C.POINTER(C.c_int64), C.POINTER(gat_stats)]),
     "gat_count": (C.c_int, [P, P, C.POINTER(gat_config), C.POINTER(C.c_uint64),
                             C.POINTER(gat_stats)]),
 }

@@ -59,11 +59,20 @@ struct DevCopy {
     int64_t lo_total = 0;
     int32_t max_degree = 0;
     bool ready = false;
+    std::vector<int64_t> lo_host;   // host copy of lo_off
+    std::vector<int64_t> off_host;  // host copy of off
     void release() {
         cudaFree(off);
         cudaFree(adj);
         cudaFree(lo_off);
-        *this = DevCopy{};
+        off = nullptr;
+        adj = nullptr;
+        lo_off = nullptr;
+        lo_total = 0;
+        max_degree = 0;
+        ready = false;
+        lo_host.clear();
+        off_host.clear();
     }
 };
 
@@ -467,6 +476,8 @@ int upload_copy(const HostGraph &h, DevCopy &d, cudaStream_t st) {
         return cuda_fail(e, "graph upload");
     }
     d.lo_total = lo[h.V];
+    d.lo_host = std::move(lo);
+    d.off_host = h.off;
     d.max_degree = h.max_degree();
     d.ready = true;
     return GAT_OK;
@@ -536,7 +547,8 @@ void gat_executor_free(gat_executor *e) { delete e; }
 namespace {
 
 int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *stream,
-               uint64_t *count, gat_stats *stats, bool balg) {
+               uint64_t *count, gat_stats *stats, bool balg, int64_t root_begin = -1,
+               int64_t root_end = -1, int shard = 0, int num_shards = 0) {
     auto t0 = std::chrono::steady_clock::now();
     if (!e || !g || !s || !count) return fail(GAT_ERR_ARGUMENT, "null argument");
     gat_stats st{};
@@ -581,6 +593,21 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
     shape.block = e->cfg.threads_per_block;
     shape.chunk = e->cfg.chunk > 0 ? e->cfg.chunk : 16;
     shape.linear_below = e->cfg.set_search_type;
+    const bool ranged = root_begin >= 0 || num_shards > 0;
+    if (num_shards > 0) {
+        if (shard < 0 || shard >= num_shards)
+            return fail(GAT_ERR_ARGUMENT, "shard index out of range");
+        const int64_t total = plan.level1_bounded ? view.lo_total : view.E;
+        shape.task_begin = total * shard / num_shards;
+        shape.task_end = total * (shard + 1) / num_shards;
+    }
+    if (root_begin >= 0) {
+        if (root_end < root_begin || root_end > view.V)
+            return fail(GAT_ERR_ARGUMENT, "root range outside [0, V]");
+        const int64_t *toff = plan.level1_bounded ? dc->lo_host.data() : dc->off_host.data();
+        shape.task_begin = toff[root_begin];
+        shape.task_end = toff[root_end];
+    }
     int occ = blocks_per_sm(shape.tile, shape.block, balg);
     if (occ <= 0) return fail(GAT_ERR_CUDA, "kernel does not fit on the device");
     shape.grid = e->cfg.num_blocks > 0 ? e->cfg.num_blocks : e->sms * occ;
@@ -620,13 +647,18 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
     if (e->host_ctr->error) return fail(GAT_ERR_DEVICE, "kernel reported an internal error");
     int64_t raw = (int64_t)e->host_ctr->result;
-    if (plan.divisor <= 0 || raw % plan.divisor != 0)
-        return fail(GAT_ERR_DEVICE, "engine total is not a multiple of the plan divisor");
-    *count = (uint64_t)(raw / plan.divisor);
+    if (ranged) {
+        *count = (uint64_t)raw;  // partial sums are divided by the caller
+    } else {
+        if (plan.divisor <= 0 || raw % plan.divisor != 0)
+            return fail(GAT_ERR_DEVICE, "engine total is not a multiple of the plan divisor");
+        *count = (uint64_t)(raw / plan.divisor);
+    }
     st.kernel_ms = ms;
     st.raw_sum = raw;
     st.divisor = plan.divisor;
-    st.tasks = plan.level1_bounded ? (uint64_t)view.lo_total : (uint64_t)view.E;
+    st.tasks = ranged ? (uint64_t)(shape.task_end - shape.task_begin)
+                      : (plan.level1_bounded ? (uint64_t)view.lo_total : (uint64_t)view.E);
     st.balg_bytes = e->host_ctr->bytes;
     st.grid = shape.grid;
     st.block = shape.block;
@@ -649,6 +681,26 @@ int gat_executor_count(gat_executor *e, gat_graph *g, const gat_schedule *s, voi
 int gat_executor_count_balg(gat_executor *e, gat_graph *g, const gat_schedule *s,
                             void *stream, uint64_t *count, gat_stats *stats) {
     return count_impl(e, g, s, stream, count, stats, true);
+}
+
+int gat_executor_count_range(gat_executor *e, gat_graph *g, const gat_schedule *s,
+                             void *stream, int32_t root_begin, int32_t root_end,
+                             int64_t *raw_sum, gat_stats *stats) {
+    if (root_begin < 0) return fail(GAT_ERR_ARGUMENT, "negative root");
+    uint64_t c = 0;
+    int rc = count_impl(e, g, s, stream, &c, stats, false, root_begin, root_end);
+    if (rc == GAT_OK && raw_sum) *raw_sum = (int64_t)c;
+    return rc;
+}
+
+int gat_executor_count_shard(gat_executor *e, gat_graph *g, const gat_schedule *s,
+                             void *stream, int32_t shard, int32_t num_shards,
+                             int64_t *raw_sum, gat_stats *stats) {
+    if (num_shards < 1) return fail(GAT_ERR_ARGUMENT, "num_shards must be >= 1");
+    uint64_t c = 0;
+    int rc = count_impl(e, g, s, stream, &c, stats, false, -1, -1, shard, num_shards);
+    if (rc == GAT_OK && raw_sum) *raw_sum = (int64_t)c;
+    return rc;
 }
 
 int gat_count(gat_graph *g, const gat_schedule *s, const gat_config *c, uint64_t *count,

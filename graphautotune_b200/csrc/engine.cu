@@ -56,7 +56,8 @@ struct SearchArgs {
     const int64_t *lo_off;
     int32_t V;
     int32_t cap;
-    int64_t num_tasks;
+    int64_t task_begin;  // first level-1 unit of this launch
+    int64_t num_tasks;   // one past the last
     DevCounters *ctr;
     int32_t *scratch;
     int64_t scratch_stride;
@@ -340,7 +341,9 @@ __global__ void __launch_bounds__(256)
 
     for (;;) {
         unsigned long long start = 0;
-        if (t.lane == 0) start = atomicAdd(&a.ctr->cursor, (unsigned long long)a.chunk);
+        if (t.lane == 0)
+            start = (unsigned long long)a.task_begin +
+                    atomicAdd(&a.ctr->cursor, (unsigned long long)a.chunk);
         start = t.bcast(start, 0);
         if (start >= (unsigned long long)a.num_tasks) break;
         const int64_t end = min((int64_t)start + a.chunk, a.num_tasks);
@@ -486,7 +489,9 @@ cudaError_t launch_search(const GatPlan *d_plan, const GatPlan &h_plan,
     a.lo_off = g.lo_off;
     a.V = g.V;
     a.cap = g.max_degree > 0 ? g.max_degree : 1;
-    a.num_tasks = h_plan.level1_bounded ? g.lo_total : g.E;
+    a.task_begin = shape.task_begin;
+    a.num_tasks = shape.task_end >= 0 ? shape.task_end
+                                      : (h_plan.level1_bounded ? g.lo_total : g.E);
     a.ctr = counters;
     a.scratch = scratch;
     a.scratch_stride = scratch_stride;

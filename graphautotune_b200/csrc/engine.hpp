@@ -27,6 +27,8 @@ struct LaunchShape {
     int tile = 32;        // lanes cooperating on one unit
     int chunk = 16;       // level-1 units taken per queue grab
     int linear_below = 0; // lists shorter than this are scanned linearly
+    int64_t task_begin = 0;  // level-1 unit range [task_begin, task_end);
+    int64_t task_end = -1;   // -1: all units
 };
 
 // Device counters used by one search: work-queue cursor, signed 64-bit

@@ -196,6 +196,24 @@ int gat_executor_count(gat_executor *e, gat_graph *g, const gat_schedule *s,
 int gat_executor_count_balg(gat_executor *e, gat_graph *g,
                             const gat_schedule *s, void *stream,
                             uint64_t *count, gat_stats *stats);
+/* Counts only the units whose first vertex v0 lies in [root_begin,
+ * root_end) (the reference's first-level chunking, engine.cuh:246-261, made
+ * an API: the unit of sampling and of sharding across GPUs).  For exact
+ * schedules on a degree-ordered upload the roots are relabelled ids.
+ * *raw_sum receives the undivided signed total; the caller sums the shards
+ * and divides by stats->divisor. */
+int gat_executor_count_range(gat_executor *e, gat_graph *g,
+                             const gat_schedule *s, void *stream,
+                             int32_t root_begin, int32_t root_end,
+                             int64_t *raw_sum, gat_stats *stats);
+/* Counts shard `shard` of `num_shards` equal slices of the level-1 work
+ * queue (balanced by units, not by vertices, so power-law rows spread
+ * evenly).  One process per GPU calls it with its rank; the shards' raw sums
+ * add up to the whole-graph raw sum (divide by stats->divisor). */
+int gat_executor_count_shard(gat_executor *e, gat_graph *g,
+                             const gat_schedule *s, void *stream,
+                             int32_t shard, int32_t num_shards,
+                             int64_t *raw_sum, gat_stats *stats);
 /* One-shot convenience: executor from config (NULL = engine default). */
 int gat_count(gat_graph *g, const gat_schedule *s, const gat_config *c,
               uint64_t *count, gat_stats *stats);

@@ -293,13 +293,63 @@ uint64_t oracle_naive_labelled(int32_t V, const int64_t *offs,
     return total;
 }
 
+uint64_t oracle_naive_labelled_strided(int32_t V, const int64_t *offs,
+                                       const int32_t *adj, const char *pattern,
+                                       int64_t first, int64_t num,
+                                       int64_t stride, int threads) {
+    CSR g{V, offs, adj};
+    Pat p(pattern);
+    if (p.n == 0 || stride < 1) return 0;
+    uint64_t total = 0;
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) \
+    num_threads(threads)
+    for (int64_t i = 0; i < num; i++) {
+        int64_t v0 = first + i * stride;
+        if (v0 < 0 || v0 >= V) continue;
+        int32_t choose[10];
+        choose[0] = (int32_t)v0;
+        total += naive_rec(g, p, 1, choose);
+    }
+    return total;
+}
+
 uint64_t oracle_backtrack_labelled(int32_t V, const int64_t *offs,
                                    const int32_t *adj, const char *pattern,
                                    int32_t root_begin, int32_t root_end,
                                    int threads) {
     CSR g{V, offs, adj};
+    Pat p0(pattern);
+    if (p0.n == 0) return 0;
+    // Relabel the pattern into breadth-first order from vertex 0 so every
+    // later vertex has an earlier neighbour (the labelled count does not
+    // depend on the labelling; the search time does).
+    int order[10], pos[10], cnt = 0;
+    bool seen[10] = {};
+    order[cnt++] = 0;
+    seen[0] = true;
+    while (cnt < p0.n) {
+        int nxt = -1;
+        for (int v = 0; v < p0.n && nxt < 0; v++)
+            if (!seen[v])
+                for (int i = 0; i < cnt; i++)
+                    if (p0.e[v][order[i]]) {
+                        nxt = v;
+                        break;
+                    }
+        if (nxt < 0)
+            for (int v = 0; v < p0.n; v++)
+                if (!seen[v]) {
+                    nxt = v;
+                    break;
+                }
+        seen[nxt] = true;
+        order[cnt++] = nxt;
+    }
+    for (int i = 0; i < p0.n; i++) pos[order[i]] = i;
     Pat p(pattern);
-    if (p.n == 0) return 0;
+    for (int i = 0; i < p0.n; i++)
+        for (int j = 0; j < p0.n; j++) p.e[pos[i]][pos[j]] = p0.e[i][j];
     root_begin = std::max(root_begin, 0);
     root_end = std::min(root_end, V);
     uint64_t total = 0;

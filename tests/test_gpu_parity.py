@@ -83,10 +83,11 @@ def test_ref_mode_matches_reference_engine_rules(gat, oracle, golden_schedules, 
     assert checked > 200 and undefined > 0
 
 
+# Sized so the exhaustive CPU enumeration finishes in seconds.
 MEDIUM = [
     ("er", (2000, 10.0), 5),
-    ("rmat", (11, 16384), 6),
-    ("ba", (3000, 4), 7),
+    ("rmat", (9, 3072), 6),
+    ("ba", (2000, 3), 7),
 ]
 NAMED = ["011101110", "0111101111011110", "0101101001011010",
          "0100110110010110110010100", "0111110111110111110111110"]
@@ -118,3 +119,34 @@ def test_medium_graphs_exact_and_ref(gat, oracle, golden_schedules, kind, params
         if st != 0:
             continue
         assert executors[0].count(g, gat.Schedule(p, "ref")).count == ref_want, (kind, p)
+
+
+def test_ref_mode_larger_rmat(gat, oracle, golden_schedules, executors):
+    """Reference-engine rules on a power-law graph with hubs (R-MAT scale 12)."""
+    g = gat.Graph.rmat(12, 1 << 15, 0.57, 0.19, 0.19, 9)
+    off, adj = g.csr()
+    for p in NAMED:
+        st, want, _ = oracle.ref_engine(off, adj, golden_schedules[p])
+        assert st == 0
+        for ex in executors[:3]:
+            assert ex.count(g, gat.Schedule(p, "ref")).count == want, p
+
+
+def test_relabelling_and_sharding_invariance(gat, executors):
+    """Size-independent properties: the exact count does not depend on the
+    vertex ids (degree-ordered vs given ids), and root-range shards sum to
+    the whole."""
+    g1 = gat.Graph.rmat(13, 1 << 16, 0.57, 0.19, 0.19, 21)
+    g2 = gat.Graph.rmat(13, 1 << 16, 0.57, 0.19, 0.19, 21)
+    g1.upload(degree_order=True)
+    g2.upload(degree_order=False)
+    V = g1.v_cnt()
+    for p in NAMED:
+        s = gat.Schedule(p, "exact")
+        a = executors[0].count(g1, s)
+        b = executors[1].count(g2, s)
+        assert a.count == b.count, p
+        bounds = [0, 1, 17, V // 3, V // 2, V - 5, V]
+        raw = sum(executors[0].count_range(g1, s, lo, hi)[0]
+                  for lo, hi in zip(bounds, bounds[1:]))
+        assert raw == a.raw_sum and raw // a.divisor == a.count, p

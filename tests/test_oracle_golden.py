@@ -1,0 +1,76 @@
+"""Pins the CPU oracle to the reference's own answers (no GPU).
+
+  * oracle naive matcher == reference naive_pm binary Answer (golden file)
+  * oracle backtracking counter == the same
+  * the reference's only numeric unit test: |{1..30} n {2,4,..,60}| = 15
+    (tests/test_vertex_set.cu:44-48,76)
+  * |Aut| == the reference Schedule's multiplicity
+  * reference-engine restatement: triangle/K4/K5 count 3x/4x/5x the
+    subgraphs and the house (P2 labelling) exactly once
+    (core/schedule.hpp:827-831 keeps only restrictions inside the basic
+    vertices; scripts/run_pattern_matching.sh:16-17 for P2)
+"""
+import numpy as np
+import pytest
+
+
+def test_intersection_pin(oracle):
+    a = np.arange(1, 31, dtype=np.int32)
+    b = np.arange(2, 61, 2, dtype=np.int32)
+    assert oracle.intersect_size(a, b) == 15
+
+
+def test_naive_and_backtrack_match_reference_binary(oracle, golden_naive, golden_graphs):
+    assert len(golden_naive) > 300
+    for e in golden_naive:
+        off, adj = golden_graphs[e["graph"]].csr()
+        want = e["naive_answer"]
+        if e["graph"] in ("er60", "k5", "k7", "rmat6", "ba60") and len(e["adj"]) <= 25:
+            assert oracle.naive_labelled(off, adj, e["adj"]) == want, e
+        assert oracle.backtrack_labelled(off, adj, e["adj"]) == want, e
+
+
+def test_automorphisms_match_reference(oracle, golden_schedules):
+    for p, sd in golden_schedules.items():
+        if sd.get("crash"):
+            continue
+        assert oracle.automorphisms(p) == sd["aut"], p
+
+
+@pytest.mark.parametrize("name,factor", [("triangle", 3), ("k4", 4), ("k5", 5), ("house_p2", 1)])
+def test_ref_engine_known_multiples(oracle, golden_naive, golden_schedules, golden_graphs,
+                                    name, factor):
+    seen = 0
+    for e in golden_naive:
+        if e["pattern"] != name:
+            continue
+        off, adj = golden_graphs[e["graph"]].csr()
+        st, tot, _ = oracle.ref_engine(off, adj, golden_schedules[e["adj"]])
+        assert st == 0
+        exact = e["naive_answer"] // oracle.automorphisms(e["adj"])
+        assert tot == factor * exact, (e["graph"], tot, exact)
+        seen += 1
+    assert seen >= 5
+
+
+def test_ref_engine_root_ranges_add_up(oracle, golden_schedules, golden_graphs):
+    off, adj = golden_graphs["er200"].csr()
+    V = len(off) - 1
+    for p in ("011101110", "0101101001011010", "0100110110010110110010100"):
+        sd = golden_schedules[p]
+        st, whole, balg = oracle.ref_engine(off, adj, sd)
+        parts = [oracle.ref_engine(off, adj, sd, roots=(lo, hi))[1]
+                 for lo, hi in ((0, 7), (7, 100), (100, V))]
+        assert st == 0 and sum(parts) == whole and balg > 0
+
+
+def test_ref_engine_flags_undefined_schedules(oracle, golden_schedules, golden_graphs):
+    off, adj = golden_graphs["k7"].csr()
+    flagged = 0
+    for p, sd in golden_schedules.items():
+        if sd.get("crash"):
+            continue
+        st, _, _ = oracle.ref_engine(off, adj, sd)
+        if sd["ub_read"]:
+            flagged += st in oracle.REF_UNDEFINED
+    assert flagged > 0

@@ -139,15 +139,78 @@ def profile_traffic() -> float | None:
 
 # ----------------------------------------------------------------- reference
 
-def naive_sample_cmd(graph_path: Path, pattern: str, first: int, num: int, stride: int,
-                     threads: int):
-    return [str(ROOT / "oracle/_ref/naive_sample"), str(graph_path), pattern, str(first),
-            str(num), str(stride), str(threads)]
+MAX_ROOT_SCANS = 200
+
+
+class _Over(Exception):
+    pass
+
+
+def naive_scans(off, adj, pattern: str, v0: int, cap: int) -> int:
+    """Full scans of V the naive matcher (target/naive_pm.cu:10-44) makes for
+    root v0: one per partial embedding of 1 .. n-1 vertices.  Raises _Over
+    past `cap`."""
+    n = int(round(len(pattern) ** 0.5))
+    nbr = [[j for j in range(n) if j != i and (pattern[i * n + j] == "1"
+                                                or pattern[j * n + i] == "1")]
+           for i in range(n)]
+    count = 0
+    emb = [v0]
+
+    def rec():
+        nonlocal count
+        count += 1
+        if count > cap:
+            raise _Over
+        k = len(emb)
+        if k == n - 1:
+            return
+        prev = [j for j in nbr[k] if j < k]
+        if not prev:
+            raise _Over  # would scan every vertex: unbounded
+        lists = [adj[off[emb[j]]:off[emb[j] + 1]] for j in prev]
+        cand = min(lists, key=len)
+        others = [set(x.tolist()) for x in lists if x is not cand]
+        for u in cand.tolist():
+            if u in emb or any(u not in s for s in others):
+                continue
+            emb.append(u)
+            rec()
+            emb.pop()
+
+    rec()
+    return count
+
+
+def sample_roots(gr, pattern: str, n_scans: int, seed: int = 12345):
+    """Seeded uniform random first vertices whose naive-matcher cost is at
+    most MAX_ROOT_SCANS scans of V (costlier roots are skipped); stops when
+    the sum of scans reaches n_scans."""
+    import numpy as np
+
+    off, adj = gr.csr()
+    V = len(off) - 1
+    rng = np.random.default_rng(seed)
+    roots, total, skipped = [], 0, 0
+    for v in rng.permutation(V):
+        if int(off[v + 1] - off[v]) + 1 > MAX_ROOT_SCANS:
+            skipped += 1
+            continue
+        try:
+            cost = naive_scans(off, adj, pattern, int(v), MAX_ROOT_SCANS)
+        except _Over:
+            skipped += 1
+            continue
+        roots.append(int(v))
+        total += cost
+        if total >= n_scans:
+            break
+    return roots, total, skipped
 
 
 def cpu_naive_sample(gr, pattern: str, aut: int, budget_s: float = 15.0) -> dict:
-    """Times the reference naive matcher on a strided sample of roots on all
-    host threads; grows the sample until it takes about budget_s."""
+    """Times the reference naive matcher on a bounded random sample of roots
+    on all host threads, sized from a calibration run to take ~budget_s."""
     threads = os.cpu_count() or 1
     V = gr.v_cnt()
     binary = ROOT / "oracle/_ref/naive_sample"
@@ -161,34 +224,51 @@ def cpu_naive_sample(gr, pattern: str, aut: int, budget_s: float = 15.0) -> dict
         import pyoracle
 
         off, adj = gr.csr()
-    num = max(threads, 8)
-    while True:
-        stride = max(1, V // num)
-        first = stride // 2
+
+    def run(roots):
         t0 = time.perf_counter()
         if use_ref:
-            out = subprocess.run(naive_sample_cmd(graph_cache_path(), pattern, first, num,
-                                                  stride, threads),
+            out = subprocess.run([str(binary), str(graph_cache_path()), pattern, "-",
+                                  str(threads)], input="\n".join(map(str, roots)) + "\n",
                                  capture_output=True, text=True, check=True).stdout.split()
-            labelled = int(out[1])
-            secs = float(out[3])
-        else:
-            labelled = pyoracle.naive_labelled_strided(off, adj, pattern, first, num, stride,
-                                                       threads)
-            secs = time.perf_counter() - t0
-        if secs >= budget_s / 4 or num >= V:
-            break
-        num = min(V, int(num * max(2.0, budget_s / max(secs, 1e-3) / 2)))
-    return {
-        "value": (labelled / aut) / secs if secs > 0 else 0.0,
-        "unit": "matches/s",
-        "cores": threads,
-        "kind": "reference" if use_ref else "port",
-        "sample": f"naive matcher, pattern {pattern}, {num} first vertices "
-                  f"v0 = {first} + i*{stride} of {V}; {labelled} labelled embeddings "
-                  f"({labelled / aut:.1f} matches) in {secs:.2f} s",
-        "seconds": secs,
-    }
+            return int(out[1]), float(out[3])
+        lab = pyoracle.naive_labelled_roots(off, adj, pattern, roots, threads)
+        return lab, time.perf_counter() - t0
+
+    scans = 4 * threads
+    roots, total, skipped = sample_roots(gr, pattern, scans)
+    labelled, secs = run(roots)
+    per_scan = secs * threads / max(total, 1)
+    scans = int(budget_s * threads / max(per_scan, 1e-6))
+    roots, total, skipped = sample_roots(gr, pattern, scans)
+    return {"run": run, "roots": roots, "total": total, "skipped": skipped, "aut": aut,
+            "threads": threads, "V": V, "kind": "reference" if use_ref else "port",
+            "pattern": pattern}
+
+
+def cpu_baseline_step(plans: list[dict]) -> dict:
+    """One timed pass of the naive matcher over every pattern's sample."""
+    matches, secs, parts = 0.0, 0.0, []
+    for p in plans:
+        labelled, s = p["run"](p["roots"])
+        matches += labelled / p["aut"]
+        secs += s
+        parts.append(f"pattern {p['pattern']}: {len(p['roots'])} seeded uniform random first "
+                     f"vertices of {p['V']} costing <= {MAX_ROOT_SCANS} scans of V each "
+                     f"({p['skipped']} costlier roots skipped), {p['total']} scans, "
+                     f"{labelled} labelled embeddings ({labelled / p['aut']:.2f} matches) in "
+                     f"{s:.2f} s")
+    return {"value": matches / secs if secs > 0 else 0.0, "unit": "matches/s",
+            "cores": plans[0]["threads"], "kind": plans[0]["kind"],
+            "sample": "naive nested-loop matcher (target/naive_pm.cu) on all host threads; "
+                      + "; ".join(parts), "seconds": secs}
+
+
+def cpu_baseline_plans(gr, budget_s: float) -> list[dict]:
+    import graphautotune_b200 as g
+
+    return [cpu_naive_sample(gr, p, g.Pattern(p).automorphisms(), budget_s / len(PATTERNS))
+            for p in PATTERNS.values()]
 
 
 def run_reference(args):
@@ -198,20 +278,16 @@ def run_reference(args):
     import graphautotune_b200 as g
 
     gr, _ = load_workload_graph(g)
-    base = cpu_naive_sample(gr, PATTERNS["k4"], 24)
-    secs_per_step = base.pop("seconds")
-    for _ in range(args.warmup):
-        pass  # the sample itself is run once per step below
-    vals = []
-    for _ in range(args.steps):
-        r = cpu_naive_sample(gr, PATTERNS["k4"], 24, budget_s=min(15.0, secs_per_step * 1.2))
-        vals.append(r["value"])
-    value = statistics.median(vals)
+    plans = cpu_baseline_plans(gr, 12.0)  # calibration = warm-up
+    steps = [cpu_baseline_step(plans) for _ in range(args.steps)]
+    value = statistics.median(s["value"] for s in steps)
+    base = dict(steps[-1])
+    secs = base.pop("seconds")
     line = {
-        "impl": "reference", "metric": "matches/s (exact 4-clique, CPU naive matcher sample)",
+        "impl": "reference", "metric": "matches/s (exact 4-clique + 4-cycle counts)",
         "value": value, "unit": "matches/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": secs_per_step * 1000,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "warmup": args.warmup, "ms_per_step": secs * 1000,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic", "config": {"workload": WORKLOAD["name"], **WORKLOAD,
                                         "patterns": list(PATTERNS)},
         "cpu_baseline": {**base, "value": value},
@@ -318,7 +394,7 @@ def run_ours(args):
         for i in range(max(1, min(3, args.steps))):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            g2 = g.Graph.from_csr(off_p.numpy(), adj_p.numpy())
+            g2 = g.Graph.from_csr(off_p.numpy(), adj_p.numpy(), check_symmetry=False)
             g2.upload(degree_order=True)
             tot = 0
             for k, s in scheds.items():
@@ -328,7 +404,7 @@ def run_ours(args):
             assert tot == matches, (tot, matches)
             del g2
         e2e_value = matches / (statistics.median(e2e_ms) / 1000.0)
-        cpu = cpu_naive_sample(gr, PATTERNS["k4"], 24)
+        cpu = cpu_baseline_step(cpu_baseline_plans(gr, 12.0))
         cpu.pop("seconds", None)
         line = {
             "metric": "matches/s (exact 4-clique + 4-cycle counts)",
@@ -365,13 +441,37 @@ def run_ours(args):
     return 0
 
 
+def run_profile_case(args):
+    """A bounded slice of one workload pattern's search, for profilers: the
+    workload graph, `pattern` counted over shard 0 of `parts` equal slices of
+    the work queue, warmup + steps launches (one search kernel each)."""
+    import torch
+
+    import graphautotune_b200 as g
+
+    name, parts = args.profile.split(":")
+    torch.cuda.set_device(0)
+    gr, _ = load_workload_graph(g)
+    gr.upload(degree_order=True)
+    ex = g.Executor(g.Config.engine_default())
+    s = g.Schedule(PATTERNS[name], "exact", stats_graph=gr)
+    for i in range(args.warmup + args.steps):
+        raw, r = ex.count_shard(gr, s, 0, int(parts))
+        log(f"{name} shard 0/{parts}: raw {raw} tasks {r.tasks} kernel {r.kernel_ms:.2f} ms")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile", default=None,
+                    help="PATTERN:PARTS, e.g. c4:16 - one slice of the search, for ncu")
     args = ap.parse_args()
+    if args.profile:
+        sys.exit(run_profile_case(args))
     from graphautotune_b200 import _lib
 
     if not _lib.LIB_PATH.exists():

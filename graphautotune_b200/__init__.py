@@ -185,12 +185,15 @@ class Graph(_Handle):
         return g
 
     @classmethod
-    def from_csr(cls, offsets: np.ndarray, adj: np.ndarray) -> "Graph":
+    def from_csr(cls, offsets: np.ndarray, adj: np.ndarray, check_symmetry: bool = True
+                 ) -> "Graph":
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         a = np.ascontiguousarray(adj, dtype=np.int32)
         g = cls()
         check(lib().gat_graph_from_csr(len(off) - 1, len(a), off.ctypes.data, a.ctypes.data,
                                        C.byref(g._h)))
+        if check_symmetry:
+            check(lib().gat_graph_validate(g._h, 1))
         return g
 
     @classmethod

@@ -401,8 +401,16 @@ int gat_graph_from_csr(int32_t V, int64_t E, const int64_t *offsets,
     g->host.off.assign(offsets, offsets + V + 1);
     g->host.adj.assign(adj, adj + E);
     std::string err;
-    if (!validate(g->host, true, &err)) return fail(GAT_ERR_ARGUMENT, "invalid CSR: " + err);
+    if (!validate(g->host, false, &err)) return fail(GAT_ERR_ARGUMENT, "invalid CSR: " + err);
     *out = g.release();
+    return GAT_OK;
+}
+
+int gat_graph_validate(const gat_graph *g, int check_symmetry) {
+    if (!g) return fail(GAT_ERR_ARGUMENT, "null argument");
+    std::string err;
+    if (!validate(g->host, check_symmetry != 0, &err))
+        return fail(GAT_ERR_ARGUMENT, "invalid CSR: " + err);
     return GAT_OK;
 }
 

@@ -142,10 +142,12 @@ int gat_config_format(const gat_config *c, char *buf, size_t cap);
  * Binary layout: int32 V, int64 E (directed entries), int64 offsets[V+1],
  * int32 neighbours[E]; text layout: "V E" then E lines "u v". */
 int gat_graph_load(const char *path, int binary, gat_graph **out);
-/* Copies caller CSR arrays (must be sorted, deduplicated, symmetric, no
- * self loops; checked). */
+/* Copies caller CSR arrays.  Rows must be strictly increasing, ids in
+ * [0, V), no self loops (checked, O(E)); the lists must also be symmetric,
+ * which gat_graph_validate(g, 1) checks in O(E log d). */
 int gat_graph_from_csr(int32_t V, int64_t E, const int64_t *offsets,
                        const int32_t *adj, gat_graph **out);
+int gat_graph_validate(const gat_graph *g, int check_symmetry);
 /* Seeded synthetic graphs (splitmix64 streams).  kind: 0 Erdos-Renyi
  * (p0 = n, p1 = avg degree), 1 R-MAT (p0 = scale, p1 = edge samples,
  * p2..p4 = a, b, c), 2 Barabasi-Albert (p0 = n, p1 = m). */

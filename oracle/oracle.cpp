@@ -293,19 +293,19 @@ uint64_t oracle_naive_labelled(int32_t V, const int64_t *offs,
     return total;
 }
 
-uint64_t oracle_naive_labelled_strided(int32_t V, const int64_t *offs,
-                                       const int32_t *adj, const char *pattern,
-                                       int64_t first, int64_t num,
-                                       int64_t stride, int threads) {
+uint64_t oracle_naive_labelled_roots(int32_t V, const int64_t *offs,
+                                     const int32_t *adj, const char *pattern,
+                                     const int32_t *roots, int64_t num,
+                                     int threads) {
     CSR g{V, offs, adj};
     Pat p(pattern);
-    if (p.n == 0 || stride < 1) return 0;
+    if (p.n == 0) return 0;
     uint64_t total = 0;
     if (threads <= 0) threads = omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) \
     num_threads(threads)
     for (int64_t i = 0; i < num; i++) {
-        int64_t v0 = first + i * stride;
+        int64_t v0 = roots[i];
         if (v0 < 0 || v0 >= V) continue;
         int32_t choose[10];
         choose[0] = (int32_t)v0;
@@ -392,9 +392,10 @@ int oracle_ref_engine(int32_t V, const int64_t *offs, const int32_t *adj,
     // Restriction ranges used by prepare_v_storage_kernel for vertices
     // 1..basic-1 must stay inside the initialised part of
     // ScheduleData::restrictions (core/schedule.hpp:1015-1021).
+    // ... and name vertices already chosen (slot k and above is stale).
     for (int k = 1; k < sd.basic; k++)
         for (int i = sd.rs[k]; i < sd.rs[k + 1]; i++)
-            if (i >= sd.R) return -2;
+            if (i >= sd.R || sd.rest[i] >= k) return -2;
     for (int k = 2; k < sd.basic; k++) {
         int p = sd.loop[k];
         if (sd.size_only[p] && sd.father[p] != -1) return -3;

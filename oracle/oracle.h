@@ -34,12 +34,12 @@ uint64_t oracle_naive_labelled(int32_t V, const int64_t *offs,
                                int32_t root_begin, int32_t root_end,
                                int threads);
 
-/* oracle_naive_labelled over the first-level vertices first + i*stride,
- * i in [0, num) (a bounded, spread-out sample of roots). */
-uint64_t oracle_naive_labelled_strided(int32_t V, const int64_t *offs,
-                                       const int32_t *adj, const char *pattern,
-                                       int64_t first, int64_t num,
-                                       int64_t stride, int threads);
+/* oracle_naive_labelled over an explicit list of first-level vertices (a
+ * bounded sample of roots). */
+uint64_t oracle_naive_labelled_roots(int32_t V, const int64_t *offs,
+                                     const int32_t *adj, const char *pattern,
+                                     const int32_t *roots, int64_t num,
+                                     int threads);
 
 /* Same count as oracle_naive_labelled, with candidates drawn from the
  * neighbour list of one earlier adjacent pattern vertex instead of all V

@@ -31,9 +31,9 @@ def lib():
         l.oracle_naive_labelled.restype = C.c_uint64
         l.oracle_naive_labelled.argtypes = [C.c_int32, i64p, i32p, C.c_char_p, C.c_int32,
                                             C.c_int32, C.c_int]
-        l.oracle_naive_labelled_strided.restype = C.c_uint64
-        l.oracle_naive_labelled_strided.argtypes = [C.c_int32, i64p, i32p, C.c_char_p,
-                                                    C.c_int64, C.c_int64, C.c_int64, C.c_int]
+        l.oracle_naive_labelled_roots.restype = C.c_uint64
+        l.oracle_naive_labelled_roots.argtypes = [C.c_int32, i64p, i32p, C.c_char_p, i32p,
+                                                  C.c_int64, C.c_int]
         l.oracle_backtrack_labelled.restype = C.c_uint64
         l.oracle_backtrack_labelled.argtypes = l.oracle_naive_labelled.argtypes
         l.oracle_automorphisms.restype = C.c_int64
@@ -61,11 +61,12 @@ def naive_labelled(off, adj, pattern: str, roots=None, threads: int = 0) -> int:
     return lib().oracle_naive_labelled(V, po, pa, pattern.encode(), b, e, threads)
 
 
-def naive_labelled_strided(off, adj, pattern: str, first: int, num: int, stride: int,
-                           threads: int = 0) -> int:
+def naive_labelled_roots(off, adj, pattern: str, roots, threads: int = 0) -> int:
     V, o, a, po, pa = _csr(off, adj)
-    return lib().oracle_naive_labelled_strided(V, po, pa, pattern.encode(), first, num,
-                                               stride, threads)
+    r = np.ascontiguousarray(roots, np.int32)
+    return lib().oracle_naive_labelled_roots(V, po, pa, pattern.encode(),
+                                             r.ctypes.data_as(C.POINTER(C.c_int32)), len(r),
+                                             threads)
 
 
 def backtrack_labelled(off, adj, pattern: str, roots=None, threads: int = 0) -> int:

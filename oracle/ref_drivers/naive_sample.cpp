@@ -14,6 +14,8 @@
 // usage: naive_sample <graph.bin> <pattern_adj> <first_v0> <num_v0> <stride>
 //                     [threads]
 //   samples v0 = first_v0 + i*stride, i in [0, num_v0), v0 < V
+//        naive_sample <graph.bin> <pattern_adj> - <threads>
+//   reads the roots (one per line) from stdin
 // prints one line: "labelled <sum> seconds <t> roots <k> threads <T>"
 #include <omp.h>
 
@@ -30,10 +32,12 @@
 #undef main
 
 int main(int argc, char **argv) {
-    if (argc < 6) {
+    bool from_stdin = argc >= 4 && std::string(argv[3]) == "-";
+    if (argc < 6 && !from_stdin) {
         std::fprintf(stderr,
-                     "usage: %s graph.bin pattern first num stride [threads]\n",
-                     argv[0]);
+                     "usage: %s graph.bin pattern first num stride [threads]\n"
+                     "       %s graph.bin pattern - [threads] < roots\n",
+                     argv[0], argv[0]);
         return 2;
     }
     std::ifstream f{argv[1], std::ios::binary};
@@ -43,15 +47,23 @@ int main(int argc, char **argv) {
     }
     Infra::GlobalMemoryGraph<default_config> g{f, true};
     Core::Pattern p{std::string(argv[2])};
-    long long first = std::atoll(argv[3]);
-    long long num = std::atoll(argv[4]);
-    long long stride = std::atoll(argv[5]);
-    int threads = argc > 6 ? std::atoi(argv[6]) : omp_get_max_threads();
     std::vector<long long> roots;
-    for (long long i = 0; i < num; i++) {
-        long long v = first + i * stride;
-        if (v >= g.v_cnt()) break;
-        roots.push_back(v);
+    int threads = omp_get_max_threads();
+    if (from_stdin) {
+        if (argc > 4) threads = std::atoi(argv[4]);
+        long long v;
+        while (std::cin >> v)
+            if (v >= 0 && v < g.v_cnt()) roots.push_back(v);
+    } else {
+        long long first = std::atoll(argv[3]);
+        long long num = std::atoll(argv[4]);
+        long long stride = std::atoll(argv[5]);
+        if (argc > 6) threads = std::atoi(argv[6]);
+        for (long long i = 0; i < num; i++) {
+            long long v = first + i * stride;
+            if (v >= g.v_cnt()) break;
+            roots.push_back(v);
+        }
     }
     long long total = 0;
     auto t0 = std::chrono::steady_clock::now();

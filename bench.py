@@ -154,6 +154,8 @@ def naive_scans(off, adj, pattern: str, v0: int, cap: int) -> int:
     nbr = [[j for j in range(n) if j != i and (pattern[i * n + j] == "1"
                                                 or pattern[j * n + i] == "1")]
            for i in range(n)]
+    import numpy as np
+
     count = 0
     emb = [v0]
 
@@ -168,12 +170,18 @@ def naive_scans(off, adj, pattern: str, v0: int, cap: int) -> int:
         prev = [j for j in nbr[k] if j < k]
         if not prev:
             raise _Over  # would scan every vertex: unbounded
-        lists = [adj[off[emb[j]]:off[emb[j] + 1]] for j in prev]
-        cand = min(lists, key=len)
-        others = [set(x.tolist()) for x in lists if x is not cand]
+        lists = sorted((adj[off[emb[j]]:off[emb[j] + 1]] for j in prev), key=len)
+        cand = lists[0]
+        for other in lists[1:]:
+            if len(cand) == 0 or len(other) == 0:
+                cand = cand[:0]
+                break
+            idx = np.minimum(np.searchsorted(other, cand), len(other) - 1)
+            cand = cand[other[idx] == cand]
+        cand = cand[~np.isin(cand, emb)]
+        if count + len(cand) > cap:  # every candidate costs at least one scan
+            raise _Over
         for u in cand.tolist():
-            if u in emb or any(u not in s for s in others):
-                continue
             emb.append(u)
             rec()
             emb.pop()

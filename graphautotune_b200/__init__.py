@@ -128,11 +128,12 @@ class Config:
     threads_per_warp: int = 1
     max_regs: int = 32
     chunk: int = 16
+    hub_bitmaps: int = 1
     memory_budget: int = 0
 
     _FIELDS = ("set_search_type", "set_intersection_type", "vertex_store_type",
                "graph_backend_type", "num_blocks", "threads_per_block",
-               "threads_per_warp", "max_regs", "chunk", "memory_budget")
+               "threads_per_warp", "max_regs", "chunk", "hub_bitmaps", "memory_budget")
 
     @classmethod
     def _from_c(cls, c: gat_config) -> "Config":
@@ -242,10 +243,24 @@ class Graph(_Handle):
                if e > 0 else np.zeros(0, np.int32))
         return off, adj
 
-    def upload(self, degree_order: bool = True, stream: int | None = None) -> None:
-        """GlobalMemoryGraph::to_device (graph_backend.cuh:102-118)."""
-        check(lib().gat_graph_upload(self._h, UPLOAD_DEGREE_ORDER if degree_order else 0,
-                                     C.c_void_p(stream) if stream else None))
+    def upload(self, degree_order: bool = True, stream: int | None = None,
+               hub_min_degree: int | None = None, hub_max_bytes: int | None = None) -> None:
+        """GlobalMemoryGraph::to_device (graph_backend.cuh:102-118), plus the
+        degree-ordered copy and hub bitmaps."""
+        flags = UPLOAD_DEGREE_ORDER if degree_order else 0
+        s = C.c_void_p(stream) if stream else None
+        if hub_min_degree is None and hub_max_bytes is None:
+            check(lib().gat_graph_upload(self._h, flags, s))
+        else:
+            check(lib().gat_graph_upload_ex(self._h, flags,
+                                            512 if hub_min_degree is None else hub_min_degree,
+                                            (1 << 30) if hub_max_bytes is None else hub_max_bytes,
+                                            s))
+
+    def hubs(self, ordered: bool = True) -> int:
+        n = C.c_int32()
+        check(lib().gat_graph_hubs(self._h, 1 if ordered else 0, C.byref(n)))
+        return n.value
 
 
 @dataclass

@@ -48,7 +48,7 @@ class gat_config(C.Structure):
         ("threads_per_warp", C.c_int32),
         ("max_regs", C.c_int32),
         ("chunk", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("hub_bitmaps", C.c_int32),
         ("memory_budget", C.c_int64),
         ("reserved", C.c_int64 * 4),
     ]
@@ -99,6 +99,8 @@ _SIGS = {
                                  C.POINTER(C.c_int32)]),
     "gat_graph_csr": (C.c_int, [P, C.POINTER(P), C.POINTER(P)]),
     "gat_graph_upload": (C.c_int, [P, C.c_int, P]),
+    "gat_graph_upload_ex": (C.c_int, [P, C.c_int, C.c_int64, C.c_int64, P]),
+    "gat_graph_hubs": (C.c_int, [P, C.c_int, C.POINTER(C.c_int32)]),
     "gat_graph_free": (None, [P]),
     "gat_executor_create": (C.c_int, [C.POINTER(gat_config), C.POINTER(P)]),
     "gat_executor_free": (None, [P]),

@@ -61,10 +61,23 @@ struct DevCopy {
     bool ready = false;
     std::vector<int64_t> lo_host;   // host copy of lo_off
     std::vector<int64_t> off_host;  // host copy of off
+    int32_t *hub_slot = nullptr;    // per vertex: bitmap row or -1
+    int32_t *hubs = nullptr;        // row -> vertex
+    uint32_t *bitmaps = nullptr;
+    int32_t nhubs = 0;
+    int64_t bitmap_words = 0;
     void release() {
         cudaFree(off);
         cudaFree(adj);
         cudaFree(lo_off);
+        cudaFree(hub_slot);
+        cudaFree(hubs);
+        cudaFree(bitmaps);
+        hub_slot = nullptr;
+        hubs = nullptr;
+        bitmaps = nullptr;
+        nhubs = 0;
+        bitmap_words = 0;
         off = nullptr;
         adj = nullptr;
         lo_off = nullptr;
@@ -242,6 +255,7 @@ void gat_config_default(gat_config *c) {
     c->threads_per_warp = 1;
     c->max_regs = 32;
     c->chunk = 16;
+    c->hub_bitmaps = 1;
     c->memory_budget = 0;
 }
 
@@ -295,6 +309,7 @@ bool set_field(gat_config *c, const std::string &key, const std::string &val) {
     if (k == "threads_per_warp") return i32(c->threads_per_warp);
     if (k == "max_regs") return i32(c->max_regs);
     if (k == "chunk") return i32(c->chunk);
+    if (k == "hub_bitmaps") return i32(c->hub_bitmaps);
     if (k == "memory_budget") {
         c->memory_budget = x;
         return true;
@@ -490,25 +505,76 @@ int upload_copy(const HostGraph &h, DevCopy &d, cudaStream_t st) {
     d.ready = true;
     return GAT_OK;
 }
+
+// Hub bitmaps for the vertices of degree >= min_degree, largest degree first,
+// as many as fit in max_bytes.
+int upload_hubs(const HostGraph &h, DevCopy &d, int64_t min_degree, int64_t max_bytes,
+                cudaStream_t st) {
+    if (min_degree <= 0 || max_bytes <= 0 || h.V == 0) return GAT_OK;
+    const int64_t words = (int64_t(h.V) + 31) / 32;
+    std::vector<int32_t> cand;
+    for (int32_t v = 0; v < h.V; v++)
+        if (h.degree(v) >= min_degree) cand.push_back(v);
+    std::stable_sort(cand.begin(), cand.end(),
+                     [&](int32_t x, int32_t y) { return h.degree(x) > h.degree(y); });
+    const int64_t fit = max_bytes / (words * 4);
+    if ((int64_t)cand.size() > fit) cand.resize(size_t(fit));
+    if (cand.empty()) return GAT_OK;
+    std::vector<int32_t> slot(size_t(h.V), -1);
+    for (size_t i = 0; i < cand.size(); i++) slot[cand[i]] = (int32_t)i;
+    cudaError_t e;
+    const size_t bm_bytes = size_t(cand.size()) * size_t(words) * 4;
+    if ((e = cudaMalloc(&d.hub_slot, sizeof(int32_t) * h.V)) != cudaSuccess ||
+        (e = cudaMalloc(&d.hubs, sizeof(int32_t) * cand.size())) != cudaSuccess ||
+        (e = cudaMalloc(&d.bitmaps, bm_bytes)) != cudaSuccess)
+        return fail(GAT_ERR_MEMORY, std::string("hub bitmap allocation: ") + cudaGetErrorString(e));
+    if ((e = cudaMemcpyAsync(d.hub_slot, slot.data(), sizeof(int32_t) * h.V,
+                             cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d.hubs, cand.data(), sizeof(int32_t) * cand.size(),
+                             cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(d.bitmaps, 0, bm_bytes, st)) != cudaSuccess ||
+        (e = build_hub_bitmaps(d.off, d.adj, d.hubs, (int32_t)cand.size(), words, d.bitmaps,
+                               st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return cuda_fail(e, "hub bitmaps");
+    d.nhubs = (int32_t)cand.size();
+    d.bitmap_words = words;
+    return GAT_OK;
+}
 }  // namespace
 
-int gat_graph_upload(gat_graph *g, int flags, void *stream) {
+int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
+                        int64_t hub_max_bytes, void *stream) {
     if (!g) return fail(GAT_ERR_ARGUMENT, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     int rc = upload_copy(g->host, g->dev, st);
+    if (rc == GAT_OK) rc = upload_hubs(g->host, g->dev, hub_min_degree, hub_max_bytes, st);
     if (rc != GAT_OK) return rc;
     if (flags & GAT_UPLOAD_DEGREE_ORDER) {
         HostGraph r;
         relabel_by_degree(g->host, r, nullptr);
         rc = upload_copy(r, g->dev_ordered, st);
+        if (rc == GAT_OK)
+            rc = upload_hubs(r, g->dev_ordered, hub_min_degree, hub_max_bytes, st);
         if (rc != GAT_OK) return rc;
     } else {
         g->dev_ordered.release();
     }
     g->device = dev;
+    return GAT_OK;
+}
+
+int gat_graph_upload(gat_graph *g, int flags, void *stream) {
+    return gat_graph_upload_ex(g, flags, GAT_HUB_MIN_DEGREE_DEFAULT, GAT_HUB_MAX_BYTES_DEFAULT,
+                               stream);
+}
+
+int gat_graph_hubs(const gat_graph *g, int ordered_copy, int32_t *nhubs) {
+    if (!g || !nhubs) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *nhubs = ordered_copy ? g->dev_ordered.nhubs : g->dev.nhubs;
     return GAT_OK;
 }
 
@@ -595,12 +661,16 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
     view.lo_off = dc->lo_off;
     view.lo_total = dc->lo_total;
     view.max_degree = dc->max_degree;
+    view.hub_slot = dc->hub_slot;
+    view.bitmaps = dc->bitmaps;
+    view.bitmap_words = dc->bitmap_words;
 
     LaunchShape shape;
     shape.tile = e->cfg.set_intersection_type == 1 ? 1 : e->cfg.threads_per_warp;
     shape.block = e->cfg.threads_per_block;
     shape.chunk = e->cfg.chunk > 0 ? e->cfg.chunk : 16;
     shape.linear_below = e->cfg.set_search_type;
+    shape.use_bitmaps = e->cfg.hub_bitmaps != 0;
     const bool ranged = root_begin >= 0 || num_shards > 0;
     if (num_shards > 0) {
         if (shard < 0 || shard >= num_shards)

@@ -30,7 +30,6 @@
 // atomicAdd on the cursor and the totals.
 #include <climits>
 #include <cstdio>
-
 #include "engine.hpp"
 
 namespace gat {
@@ -43,6 +42,7 @@ struct TileSmem {
     int32_t cnt[GAT_MAX_VERTICES];
     int32_t pos[GAT_MAX_VERTICES];
     int32_t sl[GAT_MAX_PREFIX];
+    int32_t owner[GAT_MAX_PREFIX];  // ALIAS sets: the vertex whose list it is
     int32_t pad[2];
     const int32_t *src[GAT_MAX_VERTICES];
     const int32_t *sp[GAT_MAX_PREFIX];
@@ -63,6 +63,9 @@ struct SearchArgs {
     int64_t scratch_stride;
     int32_t chunk;
     int32_t linear_below;
+    const int32_t *hub_slot;   // null: no bitmaps
+    const uint32_t *bitmaps;
+    int64_t bitmap_words;
 };
 
 template <int G>
@@ -221,6 +224,56 @@ __device__ __forceinline__ int isect_store(const Tile<G> &t, const int32_t *a,
     return n;
 }
 
+// Intersections against a hub bitmap: every element of the probe list (a
+// sorted list whose elements are all below the bitmap owner's truncation
+// bound) costs one read of the owner's row instead of a binary search.
+__device__ __forceinline__ bool bit_set(const uint32_t *row, int32_t x) {
+    return (__ldg(row + (x >> 5)) >> (x & 31)) & 1u;
+}
+
+template <int G>
+__device__ __forceinline__ int bitmap_count(const Tile<G> &t, const int32_t *probe,
+                                            int np, const uint32_t *row,
+                                            const TileSmem &S, unsigned excl) {
+    int c = 0;
+    for (int i = t.lane; i < np; i += G) {
+        const int32_t x = probe[i];
+        bool ok = bit_set(row, x);
+        unsigned m = excl;
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            ok &= (S.v[j] != x);
+        }
+        c += ok ? 1 : 0;
+    }
+    return t.sum(c);
+}
+
+template <int G>
+__device__ __forceinline__ int bitmap_store(const Tile<G> &t, const int32_t *probe,
+                                            int np, const uint32_t *row,
+                                            int32_t *out) {
+    int n = 0;
+    for (int base = 0; base < np; base += G) {
+        const int i = base + t.lane;
+        bool f = false;
+        int32_t x = 0;
+        if (i < np) {
+            x = probe[i];
+            f = bit_set(row, x);
+        }
+        const unsigned m = t.ballot(f);
+        if (f) out[n + __popc(m & ((1u << t.lane) - 1u))] = x;
+        n += __popc(m);
+    }
+    return n;
+}
+
+__device__ __forceinline__ int ceil_log2(int x) {
+    return x <= 1 ? 1 : 32 - __clz(x - 1);
+}
+
 // Builds every prefix set that ends at level k for candidate v.
 template <int G, bool STATS>
 __device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
@@ -230,14 +283,17 @@ __device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
     const int32_t *nb = a.adj + o;
     const int32_t dv = (int32_t)(a.off[v + 1] - o);
     const int pe = P.l_pbegin[k + 1];
+    const int hub_v = (a.hub_slot != nullptr) ? a.hub_slot[v] : -1;
     for (int p = P.l_pbegin[k]; p < pe; p++) {
         const int kind = P.p_kind[p];
         const int32_t *ptr = S.sp[p];
         int32_t len = 0;
+        int32_t owner = -1;
         if (!collided) {
             const int32_t T = min_of(S, P.p_trunc[p]);
             if (kind == GAT_SET_ALIAS) {
                 ptr = nb;
+                owner = v;
                 len = (T == kInf) ? dv : tile_bound<G, false>(t, nb, dv, T);
             } else {
                 const int f = P.p_father[p];
@@ -249,20 +305,46 @@ __device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
                     nl = tile_bound<G, false>(t, nb, dv, T);
                 }
                 if (STATS && t.lane == 0) bytes += 4ull * (unsigned)(nl + fl);
+                // Cheapest way to intersect: probe F into v's bitmap, probe
+                // N(v) into the bitmap of F's owner, or binary-search the
+                // shorter list in the longer one.  Both probe lists are
+                // truncated at T, which is at most F's own bound, so a bit
+                // found in the owner's full row is a member of F.
+                const int owner_f = S.owner[f];
+                const int hub_f =
+                    (a.hub_slot != nullptr && owner_f >= 0) ? a.hub_slot[owner_f] : -1;
+                const int shorter = min(nl, fl), longer = max(nl, fl);
+                const long long bs_cost = (long long)shorter * ceil_log2(longer + 1);
+                const uint32_t *row = nullptr;
+                const int32_t *probe = nullptr;
+                int np = 0;
+                if (hub_v >= 0 && (long long)fl <= bs_cost &&
+                    (hub_f < 0 || fl <= nl)) {
+                    row = a.bitmaps + (int64_t)hub_v * a.bitmap_words;
+                    probe = fp;
+                    np = fl;
+                } else if (hub_f >= 0 && (long long)nl <= bs_cost) {
+                    row = a.bitmaps + (int64_t)hub_f * a.bitmap_words;
+                    probe = nb;
+                    np = nl;
+                }
                 if (kind == GAT_SET_STORE) {
                     int32_t *out = scratch + (int64_t)P.p_slot[p] * a.cap;
-                    len = isect_store(t, nb, nl, fp, fl, out, a.linear_below);
+                    len = row ? bitmap_store(t, probe, np, row, out)
+                              : isect_store(t, nb, nl, fp, fl, out, a.linear_below);
                     ptr = out;
                     if (STATS && t.lane == 0) bytes += 4ull * (unsigned)len;
                 } else {
-                    len = isect_count(t, nb, nl, fp, fl, S, P.p_excl[p],
-                                      a.linear_below);
+                    len = row ? bitmap_count(t, probe, np, row, S, P.p_excl[p])
+                              : isect_count(t, nb, nl, fp, fl, S, P.p_excl[p],
+                                            a.linear_below);
                 }
             }
         }
         if (t.lane == 0) {
             S.sp[p] = ptr;
             S.sl[p] = len;
+            S.owner[p] = owner;
         }
         t.sync();
     }
@@ -452,7 +534,31 @@ int occupancy(int block) {
     return n;
 }
 
+// One CTA per hub (grid-stride over hubs): sets bit x of the hub's row for
+// every neighbour x.  Rows are ceil(V/32) words and every x < V.
+__global__ void __launch_bounds__(256)
+    hub_bitmap_kernel(const int64_t *off, const int32_t *adj, const int32_t *hubs,
+                      int32_t nhubs, int64_t words, uint32_t *bitmaps) {
+    for (int h = blockIdx.x; h < nhubs; h += gridDim.x) {
+        const int32_t v = hubs[h];
+        uint32_t *row = bitmaps + (int64_t)h * words;
+        for (int64_t i = off[v] + threadIdx.x; i < off[v + 1]; i += blockDim.x) {
+            const int32_t x = adj[i];
+            atomicOr(row + (x >> 5), 1u << (x & 31));
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t build_hub_bitmaps(const int64_t *off, const int32_t *adj,
+                              const int32_t *hubs, int32_t nhubs, int64_t words,
+                              uint32_t *bitmaps, cudaStream_t stream) {
+    if (nhubs <= 0) return cudaSuccess;
+    const int grid = nhubs < 4096 ? nhubs : 4096;
+    hub_bitmap_kernel<<<grid, 256, 0, stream>>>(off, adj, hubs, nhubs, words, bitmaps);
+    return cudaGetLastError();
+}
 
 size_t tile_smem_bytes() { return sizeof(TileSmem); }
 
@@ -497,6 +603,10 @@ cudaError_t launch_search(const GatPlan *d_plan, const GatPlan &h_plan,
     a.scratch_stride = scratch_stride;
     a.chunk = shape.chunk > 0 ? shape.chunk : 1;
     a.linear_below = shape.linear_below;
+    const bool hubs = shape.use_bitmaps && g.bitmaps != nullptr && g.hub_slot != nullptr;
+    a.hub_slot = hubs ? g.hub_slot : nullptr;
+    a.bitmaps = hubs ? g.bitmaps : nullptr;
+    a.bitmap_words = hubs ? g.bitmap_words : 0;
     return stats ? dispatch<true>(a, shape.tile, shape.grid, shape.block, stream)
                  : dispatch<false>(a, shape.tile, shape.grid, shape.block, stream);
 }

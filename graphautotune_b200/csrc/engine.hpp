@@ -19,7 +19,17 @@ struct DevGraphView {
     const int64_t *lo_off = nullptr;
     int64_t lo_total = 0;  // lo_off[V]
     int32_t max_degree = 0;
+    // Hub bitmaps: bit x of row hub_slot[v] is set iff x is in N(v), for
+    // the vertices with hub_slot[v] >= 0 (null when none were built).
+    const int32_t *hub_slot = nullptr;
+    const uint32_t *bitmaps = nullptr;
+    int64_t bitmap_words = 0;  // words per row = ceil(V / 32)
 };
+
+// Fills one V-bit row per hub (rows must be zeroed first).
+cudaError_t build_hub_bitmaps(const int64_t *off, const int32_t *adj,
+                              const int32_t *hubs, int32_t nhubs, int64_t words,
+                              uint32_t *bitmaps, cudaStream_t stream);
 
 struct LaunchShape {
     int grid = 0;         // CTAs
@@ -29,7 +39,9 @@ struct LaunchShape {
     int linear_below = 0; // lists shorter than this are scanned linearly
     int64_t task_begin = 0;  // level-1 unit range [task_begin, task_end);
     int64_t task_end = -1;   // -1: all units
+    bool use_bitmaps = true; // use the graph's hub bitmaps when present
 };
+
 
 // Device counters used by one search: work-queue cursor, signed 64-bit
 // total (two's complement in an unsigned word), algorithmic bytes, error

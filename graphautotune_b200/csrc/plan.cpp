@@ -47,9 +47,10 @@ void fill_common(const Structure &st, GatPlan &pl) {
         pl.p_level[p] = (int8_t)st.prefix[p].back();
         pl.p_father[p] = (int8_t)st.father[p];
     }
-    for (int k = 0; k <= st.basic; k++)
+    const int basic = std::min(st.basic, GAT_MAX_VERTICES);
+    for (int k = 0; k <= basic; k++)
         pl.l_pbegin[k] = (int8_t)st.vertex_prefix_start[k];
-    for (int k = 1; k < st.basic; k++) pl.l_loop[k] = (int8_t)st.loop_prefix[k];
+    for (int k = 1; k < basic; k++) pl.l_loop[k] = (int8_t)st.loop_prefix[k];
     pl.l_loop[0] = -1;
     for (int x = 0; x < pl.iep_num; x++)
         pl.iep_prefix[x] = (int8_t)st.iep_vertex_id[x];

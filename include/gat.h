@@ -115,7 +115,8 @@ typedef struct gat_config {
     int32_t max_regs;              /* accepted for compatibility; register
                                       use is fixed when the library is built */
     int32_t chunk;                 /* level-1 units per work-queue grab */
-    int32_t reserved0;
+    int32_t hub_bitmaps;           /* 1: intersect against the graph's hub
+                                      bitmaps where cheaper; 0: never */
     int64_t memory_budget;         /* bytes of scratch the executor may hold;
                                       0 = 4 GiB */
     int64_t reserved[4];
@@ -166,6 +167,17 @@ int gat_graph_csr(const gat_graph *g, const int64_t **offsets,
  * on vertex ids; reference-compatible counts always use the ids as given). */
 #define GAT_UPLOAD_DEGREE_ORDER 1
 int gat_graph_upload(gat_graph *g, int flags, void *stream);
+/* As gat_graph_upload, also building hub bitmaps: one V-bit row (bit x set
+ * iff x is a neighbour) for every vertex of degree >= hub_min_degree, largest
+ * degree first, as many as fit in hub_max_bytes (0 disables).
+ * gat_graph_upload uses the defaults below. */
+#define GAT_HUB_MIN_DEGREE_DEFAULT 512
+#define GAT_HUB_MAX_BYTES_DEFAULT (1LL << 30)
+int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
+                        int64_t hub_max_bytes, void *stream);
+/* Number of hub bitmaps on the given device copy (0: ids as given,
+ * 1: degree-ordered). */
+int gat_graph_hubs(const gat_graph *g, int ordered_copy, int32_t *nhubs);
 void gat_graph_free(gat_graph *g);
 
 /* -------------------------------------------------------------- engine --

@@ -132,6 +132,31 @@ def test_ref_mode_larger_rmat(gat, oracle, golden_schedules, executors):
             assert ex.count(g, gat.Schedule(p, "ref")).count == want, p
 
 
+def test_hub_bitmap_path(gat, oracle, golden_schedules, executors):
+    """Hub bitmaps built for every vertex of degree >= 4 (most of the graph):
+    exact and reference-mode counts still equal the oracle's, with and
+    without bitmaps, on both device copies."""
+    no_bm = _executor(gat, **{**CONFIGS[0], "hub_bitmaps": 0})
+    for kind, params, seed in MEDIUM:
+        g = _graph(gat, kind, params, seed)
+        g.upload(degree_order=True, hub_min_degree=4, hub_max_bytes=1 << 28)
+        assert g.hubs(True) > 0 and g.hubs(False) > 0
+        off, adj = g.csr()
+        for p in NAMED + ["0101110101010101010011000"]:
+            want = oracle.exact_count(off, adj, p)
+            s = gat.Schedule(p, "exact")
+            for ex in (executors[0], executors[1], executors[3], no_bm):
+                assert ex.count(g, s).count == want, (kind, p)
+            sd = golden_schedules.get(p)
+            if sd is None or sd.get("crash"):
+                continue
+            st, ref_want, _ = oracle.ref_engine(off, adj, sd)
+            if st != 0:
+                continue
+            for ex in (executors[0], executors[2], no_bm):
+                assert ex.count(g, gat.Schedule(p, "ref")).count == ref_want, (kind, p)
+
+
 def test_relabelling_and_sharding_invariance(gat, executors):
     """Size-independent properties: the exact count does not depend on the
     vertex ids (degree-ordered vs given ids), and root-range shards sum to

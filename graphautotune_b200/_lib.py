@@ -111,6 +111,8 @@ _SIGS = {
                                            C.POINTER(C.c_int64), C.POINTER(gat_stats)]),
     "gat_executor_count_shard": (C.c_int, [P, P, P, P, C.c_int32, C.c_int32,
                                            C.POINTER(C.c_int64), C.POINTER(gat_stats)]),
+    "gat_count_noalloc": (C.c_int, [P, P, C.c_int32, C.c_int64, C.c_int32, P,
+                                    C.POINTER(gat_config), P, P]),
     "gat_count": (C.c_int, [P, P, C.POINTER(gat_config), C.POINTER(C.c_uint64),
                             C.POINTER(gat_stats)]),
 }

@@ -781,6 +781,34 @@ int gat_executor_count_shard(gat_executor *e, gat_graph *g, const gat_schedule *
     return rc;
 }
 
+int gat_count_noalloc(const int64_t *d_offsets, const int32_t *d_adj, int32_t V, int64_t E,
+                      int32_t max_degree, const gat_schedule *s, const gat_config *c,
+                      int64_t *d_count, void *stream) {
+    if (!d_offsets || (E > 0 && !d_adj) || !s || !d_count || V < 0 || E < 0 ||
+        max_degree < 0)
+        return fail(GAT_ERR_ARGUMENT, "bad arguments");
+    if (s->trivial)
+        return fail(GAT_ERR_ARGUMENT, "patterns of at most two vertices have no device plan");
+    if (s->plan.plan.n == 0) return fail(GAT_ERR_UNDEFINED, s->plan.summary);
+    gat_config cfg;
+    if (c)
+        cfg = *c;
+    else
+        gat_config_engine_default(&cfg);
+    LaunchShape shape;
+    shape.tile = cfg.set_intersection_type == 1 ? 1 : cfg.threads_per_warp;
+    shape.block = cfg.threads_per_block;
+    shape.chunk = cfg.chunk > 0 ? cfg.chunk : 16;
+    shape.linear_below = cfg.set_search_type;
+    if (shape.block < 32 || shape.block > 256 || shape.block % 32 != 0)
+        return fail(GAT_ERR_CONFIG, "threads_per_block must be a multiple of 32 in [32, 256]");
+    std::string err;
+    int rc = count_noalloc(s->plan.plan, d_offsets, d_adj, V, E, max_degree, shape,
+                           reinterpret_cast<long long *>(d_count), (cudaStream_t)stream, &err);
+    if (rc != GAT_OK) return fail(rc, err);
+    return GAT_OK;
+}
+
 int gat_count(gat_graph *g, const gat_schedule *s, const gat_config *c, uint64_t *count,
               gat_stats *stats) {
     gat_executor *e = nullptr;

@@ -30,6 +30,10 @@
 // atomicAdd on the cursor and the totals.
 #include <climits>
 #include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "../../include/gat.h"
 #include "engine.hpp"
 
 namespace gat {
@@ -405,7 +409,10 @@ __device__ long long iep_value(const Tile<G> &t, TileSmem &S, const GatPlan &P,
     return (long long)local;
 }
 
-template <int G, bool STATS>
+// ALL_ENTRIES: the work queue is every CSR entry and units that break the
+// level-1 bound are skipped in the kernel (no lower-neighbour offset table
+// needed); used by the allocation-free entry point.
+template <int G, bool STATS, bool ALL_ENTRIES = false>
 __global__ void __launch_bounds__(256)
     search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -418,7 +425,7 @@ __global__ void __launch_bounds__(256)
     int32_t *scratch =
         a.scratch + ((int64_t)blockIdx.x * tiles_per_block + tile_in_block) *
                         a.scratch_stride;
-    const int64_t *task_off = P.level1_bounded ? a.lo_off : a.off;
+    const int64_t *task_off = (!ALL_ENTRIES && P.level1_bounded) ? a.lo_off : a.off;
     unsigned long long acc = 0, bytes = 0;
 
     for (;;) {
@@ -436,6 +443,7 @@ __global__ void __launch_bounds__(256)
             while (task_off[row + 1] <= tk) row++;
             const int32_t v0 = row;
             const int32_t v1 = a.adj[a.off[v0] + (tk - task_off[v0])];
+            if (ALL_ENTRIES && P.level1_bounded && v1 >= v0) continue;
             if (v0 != cur_v0) {
                 if (t.lane == 0) S.v[0] = v0;
                 t.sync();
@@ -609,6 +617,138 @@ cudaError_t launch_search(const GatPlan *d_plan, const GatPlan &h_plan,
     a.bitmap_words = hubs ? g.bitmap_words : 0;
     return stats ? dispatch<true>(a, shape.tile, shape.grid, shape.block, stream)
                  : dispatch<false>(a, shape.tile, shape.grid, shape.block, stream);
+}
+
+}  // namespace gat
+
+// ------------------------------------------------- allocation-free counting
+//
+// Every CUDA context that loads this library holds this array until the
+// process exits.  Layout: [0, 256) counters, [256, 2048) the device plan,
+// [2048, end) per-tile scratch for the stored prefix sets.  Host code must not
+// use the array's name as an address: its device address is obtained once
+// per device with cudaGetSymbolAddress and passed to the kernels.
+static __device__ __align__(256) unsigned char
+    gat_noalloc_scratch[GAT_NOALLOC_SCRATCH_BYTES];
+
+namespace gat {
+namespace {
+
+constexpr size_t kNoAllocPlanOffset = 256;
+constexpr size_t kNoAllocScratchOffset = 2048;
+static_assert(sizeof(DevCounters) <= kNoAllocPlanOffset, "counters fit");
+static_assert(kNoAllocPlanOffset + sizeof(GatPlan) <= kNoAllocScratchOffset, "plan fits");
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_base[256] = {};  // per device ordinal
+
+__global__ void noalloc_finish(const DevCounters *c, long long divisor, long long *out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const long long raw = (long long)c->result;
+        const bool ok = c->error == 0 && divisor > 0 && raw % divisor == 0;
+        *out = ok ? raw / divisor : LLONG_MIN;
+    }
+}
+
+template <int G>
+cudaError_t noalloc_launch(const SearchArgs &a, int block, int max_grid, int sms,
+                           cudaStream_t stream) {
+    const size_t smem = size_t(block / G) * sizeof(TileSmem);
+    cudaError_t e = cudaFuncSetAttribute(search_kernel<G, false, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         227 * 1024);
+    if (e != cudaSuccess) return e;
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_kernel<G, false, true>,
+                                                      block, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    int grid = sms * occ;
+    if (max_grid > 0 && grid > max_grid) grid = max_grid;
+    search_kernel<G, false, true><<<grid, block, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int count_noalloc(const GatPlan &plan, const int64_t *d_off, const int32_t *d_adj,
+                  int32_t V, int64_t E, int32_t max_degree, const LaunchShape &shape,
+                  long long *d_count, cudaStream_t stream, std::string *err) {
+    auto bad = [&](int code, const std::string &m) {
+        if (err) *err = m;
+        return code;
+    };
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return bad(GAT_ERR_CUDA, cudaGetErrorString(e));
+    if (dev < 0 || dev >= 256) return bad(GAT_ERR_CUDA, "device ordinal out of range");
+    unsigned char *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_base[dev]) {
+            void *p = nullptr;
+            e = cudaGetSymbolAddress(&p, gat_noalloc_scratch);
+            if (e != cudaSuccess)
+                return bad(GAT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") +
+                                             cudaGetErrorString(e));
+            g_noalloc_base[dev] = static_cast<unsigned char *>(p);
+        }
+        base = g_noalloc_base[dev];
+    }
+    const int tile = shape.tile, block = shape.block;
+    const int64_t cap = max_degree > 0 ? max_degree : 1;
+    const int64_t stride = int64_t(plan.num_store) * cap;
+    const int64_t per_block = int64_t(block / tile) * stride * int64_t(sizeof(int32_t));
+    const int64_t avail = int64_t(GAT_NOALLOC_SCRATCH_BYTES) - int64_t(kNoAllocScratchOffset);
+    int max_grid = 0;
+    if (plan.num_store > 0) {
+        if (per_block > avail)
+            return bad(GAT_ERR_MEMORY,
+                       "one CTA needs " + std::to_string(per_block) +
+                           " bytes of set scratch (tiles x stored sets x max degree x 4); "
+                           "the static scratch holds " + std::to_string(avail));
+        max_grid = (int)std::min<int64_t>(avail / per_block, 1 << 20);
+    }
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return bad(GAT_ERR_CUDA, cudaGetErrorString(e));
+    DevCounters *ctr = reinterpret_cast<DevCounters *>(base);
+    GatPlan *dplan = reinterpret_cast<GatPlan *>(base + kNoAllocPlanOffset);
+    if ((e = cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(dplan, &plan, sizeof(GatPlan), cudaMemcpyHostToDevice,
+                             stream)) != cudaSuccess)
+        return bad(GAT_ERR_CUDA, cudaGetErrorString(e));
+    SearchArgs a{};
+    a.plan = dplan;
+    a.off = d_off;
+    a.adj = d_adj;
+    a.lo_off = nullptr;
+    a.V = V;
+    a.cap = (int32_t)cap;
+    a.task_begin = 0;
+    a.num_tasks = E;
+    a.ctr = ctr;
+    a.scratch = reinterpret_cast<int32_t *>(base + kNoAllocScratchOffset);
+    a.scratch_stride = stride;
+    a.chunk = shape.chunk > 0 ? shape.chunk : 1;
+    a.linear_below = shape.linear_below;
+    a.hub_slot = nullptr;
+    a.bitmaps = nullptr;
+    a.bitmap_words = 0;
+    switch (tile) {
+        case 1: e = noalloc_launch<1>(a, block, max_grid, sms, stream); break;
+        case 2: e = noalloc_launch<2>(a, block, max_grid, sms, stream); break;
+        case 4: e = noalloc_launch<4>(a, block, max_grid, sms, stream); break;
+        case 8: e = noalloc_launch<8>(a, block, max_grid, sms, stream); break;
+        case 16: e = noalloc_launch<16>(a, block, max_grid, sms, stream); break;
+        case 32: e = noalloc_launch<32>(a, block, max_grid, sms, stream); break;
+        default: return bad(GAT_ERR_CONFIG, "threads_per_warp must be 1, 2, 4, 8, 16 or 32");
+    }
+    if (e != cudaSuccess) return bad(GAT_ERR_CUDA, cudaGetErrorString(e));
+    noalloc_finish<<<1, 32, 0, stream>>>(ctr, (long long)plan.divisor, d_count);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return bad(GAT_ERR_CUDA, cudaGetErrorString(e));
+    return GAT_OK;
 }
 
 }  // namespace gat

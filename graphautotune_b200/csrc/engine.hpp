@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 
 #include "gat_plan.h"
 
@@ -42,6 +43,14 @@ struct LaunchShape {
     bool use_bitmaps = true; // use the graph's hub bitmaps when present
 };
 
+// Counts `plan` on a caller-owned device CSR without allocating: counters,
+// plan and per-tile set scratch live in the library's static device array
+// (GAT_NOALLOC_SCRATCH_BYTES, include/gat.h).  Writes the count (raw sum /
+// divisor, or LLONG_MIN on a device-side error) to d_count on `stream`.
+// Returns a gat_status.
+int count_noalloc(const GatPlan &plan, const int64_t *d_off, const int32_t *d_adj,
+                  int32_t V, int64_t E, int32_t max_degree, const LaunchShape &shape,
+                  long long *d_count, cudaStream_t stream, std::string *err);
 
 // Device counters used by one search: work-queue cursor, signed 64-bit
 // total (two's complement in an unsigned word), algorithmic bytes, error

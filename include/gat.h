@@ -228,6 +228,32 @@ int gat_executor_count_shard(gat_executor *e, gat_graph *g,
                              const gat_schedule *s, void *stream,
                              int32_t shard, int32_t num_shards,
                              int64_t *raw_sum, gat_stats *stats);
+/* ------------------------------------------------------ allocation-free --
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they count: a host framework whose caching allocator already
+ * owns the device's memory (a cudaMalloc next to it fails or fragments the
+ * pool), a latency-critical stream that must not pick up the implicit device
+ * synchronisation cudaMalloc/cudaFree bring, or a deployment whose device
+ * memory is fixed before the first request.  The graph stays in the caller's
+ * device memory (int64 offsets[V+1], int32 neighbours[E], sorted
+ * deduplicated rows, ids as given); set scratch, counters and the plan live
+ * in one static device array of GAT_NOALLOC_SCRATCH_BYTES that every device
+ * loading this library holds until the process exits.  The grid is shrunk
+ * until every resident tile's stored sets (stored prefixes x max_degree
+ * ints) fit in the array; a schedule whose single CTA would not fit is
+ * rejected with GAT_ERR_MEMORY.  Hub bitmaps are not used.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture
+ * on the device.  Every call reuses the same array, so calls whose work
+ * overlaps on the GPU (other streams, other host threads) race and return
+ * wrong counts: serialise them.  *d_count (device memory, written in order on
+ * `stream`) receives the count gat_executor_count would return, or
+ * INT64_MIN if the kernel reported an internal error.  Nothing in this call
+ * allocates (no cudaMalloc/cudaFree, no allocating library routine). */
+#define GAT_NOALLOC_SCRATCH_BYTES (64u << 20)
+int gat_count_noalloc(const int64_t *d_offsets, const int32_t *d_adj, int32_t V,
+                      int64_t E, int32_t max_degree, const gat_schedule *s,
+                      const gat_config *c, int64_t *d_count, void *stream);
 /* One-shot convenience: executor from config (NULL = engine default). */
 int gat_count(gat_graph *g, const gat_schedule *s, const gat_config *c,
               uint64_t *count, gat_stats *stats);

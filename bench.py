@@ -374,14 +374,13 @@ def run_ours(args):
     wall = time.perf_counter() - wall0
     clocks = sampler.stop()
 
-    # totals over ranks
-    raw_vec = torch.tensor([raws[k][0] for k in PATTERNS], dtype=torch.int64, device="cuda")
-    t_vec = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(raw_vec)
-        dist.all_reduce(t_vec, op=dist.ReduceOp.MAX)
-    counts = {k: int(raw_vec[i].item()) // raws[k][1] for i, k in enumerate(PATTERNS)}
-    ms_per_step = float(t_vec.item()) / args.steps
+    # totals over ranks: sum of raw shard totals, max of device time
+    from graphautotune_b200.dist import reduce_shards
+
+    cnt_list, max_ms = reduce_shards([raws[k][0] for k in PATTERNS],
+                                     [raws[k][1] for k in PATTERNS], dev_ms, device="cuda")
+    counts = dict(zip(PATTERNS, cnt_list))
+    ms_per_step = max_ms / args.steps
     matches = sum(counts.values())
     value = matches / (ms_per_step / 1000.0)
 

@@ -328,3 +328,42 @@ class Executor(_Handle):
     def perform_search(self, graph: Graph, schedule: Schedule) -> int:
         """long long Executor::perform_search(DeviceContext&)."""
         return self.count(graph, schedule).count
+
+
+class Batch(_Handle):
+    """Many (schedule, graph) counts in one persistent launch (gat_batch_*)."""
+
+    _free = "gat_batch_free"
+
+    def __init__(self):
+        super().__init__()
+        check(lib().gat_batch_create(C.byref(self._h)))
+        self._keep: list = []  # graphs and schedules must outlive the batch
+
+    def add(self, graph: Graph, schedule: Schedule) -> int:
+        j = C.c_int32()
+        check(lib().gat_batch_add(self._h, graph._h, schedule._h, C.byref(j)))
+        self._keep.append((graph, schedule))
+        return j.value
+
+    def prepare(self, config: Config | None = None, cuda_graph: bool = True) -> None:
+        cfg = (config or Config.engine_default()).to_c()
+        check(lib().gat_batch_prepare(self._h, C.byref(cfg), 1 if cuda_graph else 0))
+
+    def run(self) -> CountResult:
+        st = gat_stats()
+        check(lib().gat_batch_run(self._h, C.byref(st)))
+        return CountResult(0, st.kernel_ms, st.total_ms, 0, 1, st.tasks, 0, st.grid, st.block,
+                           st.tile, st.scratch_bytes)
+
+    def counts(self) -> list[int]:
+        n = lib().gat_batch_size(self._h)
+        arr = (C.c_uint64 * max(n, 1))()
+        check(lib().gat_batch_counts(self._h, arr, n))
+        out = []
+        for (g, s), v in zip(self._keep, arr[:n]):
+            out.append(v - (1 << 64) if s.mode == MODE_REF_COMPAT and v >= 1 << 63 else v)
+        return out
+
+    def __len__(self) -> int:
+        return lib().gat_batch_size(self._h)

@@ -781,6 +781,253 @@ int gat_executor_count_shard(gat_executor *e, gat_graph *g, const gat_schedule *
     return rc;
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------------ batch
+
+struct gat_batch {
+    struct Job {
+        gat_graph *g;
+        const gat_schedule *s;
+    };
+    std::vector<Job> jobs;
+    gat_config cfg{};
+    bool prepared = false, use_graph = false;
+    int tile = 32, block = 256, grid = 0, chunk = 8;
+    int64_t vtotal = 0, stride = 0;
+    GatPlan *d_plans = nullptr;
+    void *d_jobs = nullptr;
+    int64_t *d_vstart = nullptr;
+    unsigned long long *d_cursor = nullptr, *d_results = nullptr, *h_results = nullptr;
+    int32_t *d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<int64_t> divisors;
+    std::vector<int> modes;
+    std::vector<int64_t> raw;
+    void release_device() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        cudaFree(d_plans);
+        cudaFree(d_jobs);
+        cudaFree(d_vstart);
+        cudaFree(d_cursor);
+        cudaFree(d_results);
+        cudaFree(d_scratch);
+        cudaFreeHost(h_results);
+        d_plans = nullptr;
+        d_jobs = nullptr;
+        d_vstart = nullptr;
+        d_cursor = nullptr;
+        d_results = nullptr;
+        d_scratch = nullptr;
+        h_results = nullptr;
+        scratch_bytes = 0;
+        prepared = false;
+    }
+    ~gat_batch() {
+        release_device();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+extern "C" {
+
+int gat_batch_create(gat_batch **out) {
+    if (!out) return fail(GAT_ERR_ARGUMENT, "null argument");
+    auto b = std::make_unique<gat_batch>();
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&b->ev0)) != cudaSuccess ||
+        (e = cudaEventCreate(&b->ev1)) != cudaSuccess)
+        return cuda_fail(e, "batch stream");
+    *out = b.release();
+    return GAT_OK;
+}
+
+void gat_batch_free(gat_batch *b) { delete b; }
+
+int gat_batch_add(gat_batch *b, gat_graph *g, const gat_schedule *s, int32_t *job_index) {
+    if (!b || !g || !s) return fail(GAT_ERR_ARGUMENT, "null argument");
+    if (s->trivial) return fail(GAT_ERR_ARGUMENT, "patterns of at most two vertices have no plan");
+    if (s->plan.plan.n == 0) return fail(GAT_ERR_UNDEFINED, s->plan.summary);
+    b->jobs.push_back({g, s});
+    b->prepared = false;
+    if (job_index) *job_index = (int32_t)b->jobs.size() - 1;
+    return GAT_OK;
+}
+
+int gat_batch_prepare(gat_batch *b, const gat_config *c, int use_cuda_graph) {
+    if (!b) return fail(GAT_ERR_ARGUMENT, "null argument");
+    if (b->jobs.empty()) return fail(GAT_ERR_STATE, "empty batch");
+    b->release_device();
+    if (c)
+        b->cfg = *c;
+    else
+        gat_config_engine_default(&b->cfg);
+    b->tile = b->cfg.set_intersection_type == 1 ? 1 : b->cfg.threads_per_warp;
+    b->block = b->cfg.threads_per_block;
+    b->chunk = b->cfg.chunk > 0 ? b->cfg.chunk : 8;
+    if (b->block < 32 || b->block > 256 || b->block % 32 || b->block % b->tile)
+        return fail(GAT_ERR_CONFIG, "bad threads_per_block / threads_per_warp");
+    const size_t J = b->jobs.size();
+    const size_t jb = batch_job_bytes();
+    std::vector<unsigned char> host_jobs(J * jb);
+    std::vector<GatPlan> plans(J);
+    std::vector<int64_t> vstart(J);
+    b->divisors.assign(J, 1);
+    b->modes.assign(J, 0);
+    cudaError_t e;
+    if ((e = cudaMalloc(&b->d_plans, sizeof(GatPlan) * J)) != cudaSuccess)
+        return fail(GAT_ERR_MEMORY, "batch plans");
+    int64_t stride = 0, vt = 0;
+    for (size_t j = 0; j < J; j++) {
+        gat_graph *g = b->jobs[j].g;
+        const gat_schedule *s = b->jobs[j].s;
+        const bool exact = s->mode == GAT_MODE_EXACT;
+        if (!g->dev.ready || (exact && !g->dev_ordered.ready)) {
+            int rc = gat_graph_upload(g, exact ? GAT_UPLOAD_DEGREE_ORDER : 0, b->stream);
+            if (rc != GAT_OK) return rc;
+        }
+        const DevCopy &dc = (exact && g->dev_ordered.ready) ? g->dev_ordered : g->dev;
+        DevGraphView v;
+        v.V = g->host.V;
+        v.E = g->host.E;
+        v.off = dc.off;
+        v.adj = dc.adj;
+        v.lo_off = dc.lo_off;
+        v.lo_total = dc.lo_total;
+        v.max_degree = dc.max_degree;
+        v.hub_slot = dc.hub_slot;
+        v.bitmaps = dc.bitmaps;
+        v.bitmap_words = dc.bitmap_words;
+        plans[j] = s->plan.plan;
+        batch_fill_job(host_jobs.data() + j * jb, b->d_plans + j, plans[j], v,
+                       b->cfg.set_search_type, b->cfg.hub_bitmaps != 0);
+        stride = std::max<int64_t>(stride, tile_scratch_ints(plans[j], v.max_degree));
+        vstart[j] = vt;
+        const int64_t n = batch_job_tasks(host_jobs.data() + j * jb);
+        vt += (n + b->chunk - 1) / b->chunk * b->chunk;
+        b->divisors[j] = plans[j].divisor;
+        b->modes[j] = s->mode;
+    }
+    b->vtotal = vt;
+    b->stride = stride;
+    int occ = batch_blocks_per_sm(b->tile, b->block);
+    if (occ <= 0) return fail(GAT_ERR_CUDA, "batch kernel does not fit on the device");
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    b->grid = b->cfg.num_blocks > 0 ? b->cfg.num_blocks : sms * occ;
+    const int64_t per_block = int64_t(b->block / b->tile) * stride * 4;
+    const int64_t budget = b->cfg.memory_budget > 0 ? b->cfg.memory_budget : (int64_t(4) << 30);
+    if (per_block > 0) {
+        if (per_block > budget) return fail(GAT_ERR_MEMORY, "memory budget below one CTA's scratch");
+        b->grid = (int)std::min<int64_t>(b->grid, budget / per_block);
+    }
+    b->scratch_bytes = size_t(std::max<int64_t>(per_block * b->grid, 4));
+    if ((e = cudaMalloc(&b->d_jobs, J * jb)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_vstart, sizeof(int64_t) * J)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_cursor, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_results, sizeof(unsigned long long) * J)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_scratch, b->scratch_bytes)) != cudaSuccess ||
+        (e = cudaMallocHost(&b->h_results, sizeof(unsigned long long) * J)) != cudaSuccess)
+        return fail(GAT_ERR_MEMORY, std::string("batch tables: ") + cudaGetErrorString(e));
+    if ((e = cudaMemcpyAsync(b->d_plans, plans.data(), sizeof(GatPlan) * J,
+                             cudaMemcpyHostToDevice, b->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(b->d_jobs, host_jobs.data(), J * jb, cudaMemcpyHostToDevice,
+                             b->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(b->d_vstart, vstart.data(), sizeof(int64_t) * J,
+                             cudaMemcpyHostToDevice, b->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(b->stream)) != cudaSuccess)
+        return cuda_fail(e, "batch upload");
+    b->use_graph = use_cuda_graph != 0;
+    if (b->use_graph) {
+        if ((e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) !=
+            cudaSuccess)
+            return cuda_fail(e, "begin capture");
+        cudaMemsetAsync(b->d_cursor, 0, sizeof(unsigned long long), b->stream);
+        cudaMemsetAsync(b->d_results, 0, sizeof(unsigned long long) * J, b->stream);
+        cudaError_t le = launch_batch(b->d_jobs, b->d_vstart, (int32_t)J, b->vtotal, b->tile,
+                                      b->grid, b->block, b->chunk, b->d_cursor, b->d_results,
+                                      b->d_scratch, b->stride, b->stream);
+        cudaMemcpyAsync(b->h_results, b->d_results, sizeof(unsigned long long) * J,
+                        cudaMemcpyDeviceToHost, b->stream);
+        e = cudaStreamEndCapture(b->stream, &b->graph);
+        if (le != cudaSuccess) return cuda_fail(le, "batch launch (capture)");
+        if (e != cudaSuccess) return cuda_fail(e, "end capture");
+        if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess)
+            return cuda_fail(e, "graph instantiate");
+    }
+    b->prepared = true;
+    return GAT_OK;
+}
+
+int gat_batch_run(gat_batch *b, gat_stats *stats) {
+    if (!b) return fail(GAT_ERR_ARGUMENT, "null argument");
+    if (!b->prepared) return fail(GAT_ERR_STATE, "batch not prepared");
+    auto t0 = std::chrono::steady_clock::now();
+    const size_t J = b->jobs.size();
+    cudaError_t e;
+    cudaEventRecord(b->ev0, b->stream);
+    if (b->use_graph) {
+        e = cudaGraphLaunch(b->exec, b->stream);
+    } else {
+        cudaMemsetAsync(b->d_cursor, 0, sizeof(unsigned long long), b->stream);
+        cudaMemsetAsync(b->d_results, 0, sizeof(unsigned long long) * J, b->stream);
+        e = launch_batch(b->d_jobs, b->d_vstart, (int32_t)J, b->vtotal, b->tile, b->grid,
+                         b->block, b->chunk, b->d_cursor, b->d_results, b->d_scratch, b->stride,
+                         b->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->h_results, b->d_results, sizeof(unsigned long long) * J,
+                                cudaMemcpyDeviceToHost, b->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+    cudaEventRecord(b->ev1, b->stream);
+    if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return cuda_fail(e, "batch run");
+    b->raw.assign(J, 0);
+    for (size_t j = 0; j < J; j++) {
+        b->raw[j] = (int64_t)b->h_results[j];
+        if (b->divisors[j] <= 0 || b->raw[j] % b->divisors[j] != 0)
+            return fail(GAT_ERR_DEVICE, "job total is not a multiple of its plan divisor");
+    }
+    if (stats) {
+        gat_stats st{};
+        float ms = 0;
+        cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+        st.kernel_ms = ms;
+        st.total_ms = std::chrono::duration<double, std::milli>(
+                          std::chrono::steady_clock::now() - t0)
+                          .count();
+        st.grid = b->grid;
+        st.block = b->block;
+        st.tile = b->tile;
+        st.launches = 1;
+        st.tasks = (uint64_t)b->vtotal;
+        st.scratch_bytes = (int64_t)b->scratch_bytes;
+        *stats = st;
+    }
+    return GAT_OK;
+}
+
+int gat_batch_counts(const gat_batch *b, uint64_t *counts, size_t n) {
+    if (!b || !counts) return fail(GAT_ERR_ARGUMENT, "null argument");
+    if (b->raw.size() != b->jobs.size()) return fail(GAT_ERR_STATE, "batch has not run");
+    if (n < b->jobs.size()) return fail(GAT_ERR_ARGUMENT, "output too small");
+    for (size_t j = 0; j < b->jobs.size(); j++)
+        counts[j] = (uint64_t)(b->raw[j] / b->divisors[j]);
+    return GAT_OK;
+}
+
+int gat_batch_size(const gat_batch *b) { return b ? (int)b->jobs.size() : 0; }
+
 int gat_count_noalloc(const int64_t *d_offsets, const int32_t *d_adj, int32_t V, int64_t E,
                       int32_t max_degree, const gat_schedule *s, const gat_config *c,
                       int64_t *d_count, void *stream) {

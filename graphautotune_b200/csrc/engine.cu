@@ -30,6 +30,7 @@
 // atomicAdd on the cursor and the totals.
 #include <climits>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -70,6 +71,12 @@ struct SearchArgs {
     const int32_t *hub_slot;   // null: no bitmaps
     const uint32_t *bitmaps;
     int64_t bitmap_words;
+};
+
+// One job of a batched launch: a plan on a graph (ctr, scratch, chunk and
+// task_begin of `args` are unused; the batch supplies them).
+struct BatchJob {
+    SearchArgs args;
 };
 
 template <int G>
@@ -303,35 +310,44 @@ __device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
                 const int f = P.p_father[p];
                 const int32_t *fp = S.sp[f];
                 int32_t fl = S.sl[f];
-                int32_t nl = dv;
-                if (T != kInf) {
+                // F is already cut at its own bound; cut again only when this
+                // set's bound is a different expression.
+                if (T != kInf && P.p_trunc[p] != P.p_trunc[f])
                     fl = tile_bound<G, false>(t, fp, fl, T);
-                    nl = tile_bound<G, false>(t, nb, dv, T);
-                }
-                if (STATS && t.lane == 0) bytes += 4ull * (unsigned)(nl + fl);
                 // Cheapest way to intersect: probe F into v's bitmap, probe
                 // N(v) into the bitmap of F's owner, or binary-search the
-                // shorter list in the longer one.  Both probe lists are
-                // truncated at T, which is at most F's own bound, so a bit
-                // found in the owner's full row is a member of F.
+                // shorter list in the longer one.  Probe lists are cut at T,
+                // which is at most F's own bound, so a bit found in the
+                // owner's full row is a member of F.  Probing F into v's row
+                // when F is no longer than N(v) needs no cut of N(v) at all.
                 const int owner_f = S.owner[f];
                 const int hub_f =
                     (a.hub_slot != nullptr && owner_f >= 0) ? a.hub_slot[owner_f] : -1;
-                const int shorter = min(nl, fl), longer = max(nl, fl);
-                const long long bs_cost = (long long)shorter * ceil_log2(longer + 1);
                 const uint32_t *row = nullptr;
                 const int32_t *probe = nullptr;
                 int np = 0;
-                if (hub_v >= 0 && (long long)fl <= bs_cost &&
-                    (hub_f < 0 || fl <= nl)) {
+                int32_t nl = dv;
+                if (hub_v >= 0 && fl <= dv) {
                     row = a.bitmaps + (int64_t)hub_v * a.bitmap_words;
                     probe = fp;
                     np = fl;
-                } else if (hub_f >= 0 && (long long)nl <= bs_cost) {
-                    row = a.bitmaps + (int64_t)hub_f * a.bitmap_words;
-                    probe = nb;
-                    np = nl;
+                    if (STATS && T != kInf) nl = tile_bound<G, false>(t, nb, dv, T);
+                } else {
+                    if (T != kInf) nl = tile_bound<G, false>(t, nb, dv, T);
+                    const int shorter = min(nl, fl), longer = max(nl, fl);
+                    const long long bs_cost = (long long)shorter * ceil_log2(longer + 1);
+                    if (hub_v >= 0 && (long long)fl <= bs_cost &&
+                        (hub_f < 0 || fl <= nl)) {
+                        row = a.bitmaps + (int64_t)hub_v * a.bitmap_words;
+                        probe = fp;
+                        np = fl;
+                    } else if (hub_f >= 0 && (long long)nl <= bs_cost) {
+                        row = a.bitmaps + (int64_t)hub_f * a.bitmap_words;
+                        probe = nb;
+                        np = nl;
+                    }
                 }
+                if (STATS && t.lane == 0) bytes += 4ull * (unsigned)(nl + fl);
                 if (kind == GAT_SET_STORE) {
                     int32_t *out = scratch + (int64_t)P.p_slot[p] * a.cap;
                     len = row ? bitmap_store(t, probe, np, row, out)
@@ -409,9 +425,77 @@ __device__ long long iep_value(const Tile<G> &t, TileSmem &S, const GatPlan &P,
     return (long long)local;
 }
 
-// ALL_ENTRIES: the work queue is every CSR entry and units that break the
-// level-1 bound are skipped in the kernel (no lower-neighbour offset table
-// needed); used by the allocation-free entry point.
+// Runs the level-1 units [start, end) of one job: each unit (v0, v1) is the
+// start of a depth-first walk over levels 2 .. basic-1.  Lane 0 of the tile
+// accumulates the units' IEP values in `acc`.
+// ALL_ENTRIES: units are numbered by CSR entry even when the plan bounds
+// v1 < v0, and the units that break the bound are skipped here (no
+// lower-neighbour offset table needed); used by the allocation-free path.
+template <int G, bool STATS, bool ALL_ENTRIES>
+__device__ __forceinline__ void run_units(const Tile<G> &t, TileSmem &S, const GatPlan &P,
+                                          const SearchArgs &a, int64_t start, int64_t end,
+                                          int32_t *scratch, unsigned long long &acc,
+                                          unsigned long long &bytes) {
+    const int basic = P.basic;
+    const int64_t *task_off = (!ALL_ENTRIES && P.level1_bounded) ? a.lo_off : a.off;
+    int32_t row = tile_bound<G, true, int64_t>(t, task_off, a.V + 1, start) - 1;
+    int32_t cur_v0 = -1;
+    for (int64_t tk = start; tk < end; tk++) {
+        while (task_off[row + 1] <= tk) row++;
+        const int32_t v0 = row;
+        const int32_t v1 = a.adj[a.off[v0] + (tk - task_off[v0])];
+        if (ALL_ENTRIES && P.level1_bounded && v1 >= v0) continue;
+        if (v0 != cur_v0) {
+            if (t.lane == 0) S.v[0] = v0;
+            t.sync();
+            level_sets<G, STATS>(t, S, P, a, 0, v0, false, scratch, bytes);
+            cur_v0 = v0;
+        }
+        if (t.lane == 0) S.v[1] = v1;
+        t.sync();
+        level_sets<G, STATS>(t, S, P, a, 1, v1, false, scratch, bytes);
+        if (basic == 2) {
+            const long long r = iep_value(t, S, P, a.linear_below);
+            if (t.lane == 0) acc += (unsigned long long)r;
+            t.sync();
+            continue;
+        }
+        setup_level(t, S, P, 2);
+        int k = 2;
+        while (k >= 2) {
+            if (S.pos[k] >= S.cnt[k]) {
+                k--;
+                continue;
+            }
+            const int32_t cand = S.src[k][S.pos[k]];
+            bool hit = false;
+            unsigned dm = P.l_distinct[k];
+            while (dm) {
+                const int j = __ffs(dm) - 1;
+                dm &= dm - 1;
+                hit |= (S.v[j] == cand);
+            }
+            t.sync();
+            if (t.lane == 0) S.pos[k]++;
+            if (hit && !P.collide_clear) {
+                t.sync();
+                continue;
+            }
+            if (t.lane == 0) S.v[k] = cand;
+            t.sync();
+            level_sets<G, STATS>(t, S, P, a, k, cand, hit, scratch, bytes);
+            if (k == basic - 1) {
+                const long long r = iep_value(t, S, P, a.linear_below);
+                if (t.lane == 0) acc += (unsigned long long)r;
+                t.sync();
+                continue;
+            }
+            setup_level(t, S, P, k + 1);
+            k++;
+        }
+    }
+}
+
 template <int G, bool STATS, bool ALL_ENTRIES = false>
 __global__ void __launch_bounds__(256)
     search_kernel(const SearchArgs a) {
@@ -421,13 +505,10 @@ __global__ void __launch_bounds__(256)
     const int tile_in_block = threadIdx.x / G;
     TileSmem &S = reinterpret_cast<TileSmem *>(smem_raw)[tile_in_block];
     const GatPlan &P = *a.plan;
-    const int basic = P.basic;
     int32_t *scratch =
         a.scratch + ((int64_t)blockIdx.x * tiles_per_block + tile_in_block) *
                         a.scratch_stride;
-    const int64_t *task_off = (!ALL_ENTRIES && P.level1_bounded) ? a.lo_off : a.off;
     unsigned long long acc = 0, bytes = 0;
-
     for (;;) {
         unsigned long long start = 0;
         if (t.lane == 0)
@@ -436,68 +517,54 @@ __global__ void __launch_bounds__(256)
         start = t.bcast(start, 0);
         if (start >= (unsigned long long)a.num_tasks) break;
         const int64_t end = min((int64_t)start + a.chunk, a.num_tasks);
-        int32_t row =
-            tile_bound<G, true, int64_t>(t, task_off, a.V + 1, (int64_t)start) - 1;
-        int32_t cur_v0 = -1;
-        for (int64_t tk = (int64_t)start; tk < end; tk++) {
-            while (task_off[row + 1] <= tk) row++;
-            const int32_t v0 = row;
-            const int32_t v1 = a.adj[a.off[v0] + (tk - task_off[v0])];
-            if (ALL_ENTRIES && P.level1_bounded && v1 >= v0) continue;
-            if (v0 != cur_v0) {
-                if (t.lane == 0) S.v[0] = v0;
-                t.sync();
-                level_sets<G, STATS>(t, S, P, a, 0, v0, false, scratch, bytes);
-                cur_v0 = v0;
-            }
-            if (t.lane == 0) S.v[1] = v1;
-            t.sync();
-            level_sets<G, STATS>(t, S, P, a, 1, v1, false, scratch, bytes);
-            if (basic == 2) {
-                const long long r = iep_value(t, S, P, a.linear_below);
-                if (t.lane == 0) acc += (unsigned long long)r;
-                t.sync();
-                continue;
-            }
-            setup_level(t, S, P, 2);
-            int k = 2;
-            while (k >= 2) {
-                if (S.pos[k] >= S.cnt[k]) {
-                    k--;
-                    continue;
-                }
-                const int32_t cand = S.src[k][S.pos[k]];
-                bool hit = false;
-                unsigned dm = P.l_distinct[k];
-                while (dm) {
-                    const int j = __ffs(dm) - 1;
-                    dm &= dm - 1;
-                    hit |= (S.v[j] == cand);
-                }
-                t.sync();
-                if (t.lane == 0) S.pos[k]++;
-                if (hit && !P.collide_clear) {
-                    t.sync();
-                    continue;
-                }
-                if (t.lane == 0) S.v[k] = cand;
-                t.sync();
-                level_sets<G, STATS>(t, S, P, a, k, cand, hit, scratch, bytes);
-                if (k == basic - 1) {
-                    const long long r = iep_value(t, S, P, a.linear_below);
-                    if (t.lane == 0) acc += (unsigned long long)r;
-                    t.sync();
-                    continue;
-                }
-                setup_level(t, S, P, k + 1);
-                k++;
-            }
-        }
+        run_units<G, STATS, ALL_ENTRIES>(t, S, P, a, (int64_t)start, end, scratch, acc,
+                                         bytes);
     }
     if (t.lane == 0) {
         atomicAdd(&a.ctr->result, acc);
         if (STATS) atomicAdd(&a.ctr->bytes, bytes);
     }
+}
+
+// Many (pattern, graph) jobs in one persistent launch.  Job j owns the
+// virtual unit range [vstart[j], vstart[j] + its units rounded up to a whole
+// chunk), so a chunk never straddles two jobs; one atomic cursor walks the
+// concatenated ranges.  A tile adds its running total to the job's result
+// whenever it moves to another job, and at exit.
+template <int G>
+__global__ void __launch_bounds__(256)
+    batch_kernel(const BatchJob *__restrict__ jobs, const int64_t *__restrict__ vstart,
+                 int32_t num_jobs, int64_t vtotal, int32_t chunk,
+                 unsigned long long *cursor, unsigned long long *results,
+                 int32_t *scratch_all, int64_t scratch_stride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Tile<G> t;
+    const int tiles_per_block = blockDim.x / G;
+    const int tile_in_block = threadIdx.x / G;
+    TileSmem &S = reinterpret_cast<TileSmem *>(smem_raw)[tile_in_block];
+    int32_t *scratch =
+        scratch_all + ((int64_t)blockIdx.x * tiles_per_block + tile_in_block) * scratch_stride;
+    unsigned long long acc = 0, bytes = 0;
+    int cur_job = -1;
+    for (;;) {
+        unsigned long long vs = 0;
+        if (t.lane == 0) vs = atomicAdd(cursor, (unsigned long long)chunk);
+        vs = t.bcast(vs, 0);
+        if (vs >= (unsigned long long)vtotal) break;
+        const int j = tile_bound<G, true, int64_t>(t, vstart, num_jobs, (int64_t)vs) - 1;
+        const BatchJob &job = jobs[j];
+        const int64_t start = (int64_t)vs - vstart[j];
+        if (start >= job.args.num_tasks) continue;  // padding of the job's last chunk
+        if (j != cur_job) {
+            if (t.lane == 0 && cur_job >= 0 && acc) atomicAdd(&results[cur_job], acc);
+            acc = 0;
+            cur_job = j;
+        }
+        const int64_t end = min(start + chunk, job.args.num_tasks);
+        run_units<G, false, false>(t, S, *job.args.plan, job.args, start, end, scratch, acc,
+                                   bytes);
+    }
+    if (t.lane == 0 && cur_job >= 0 && acc) atomicAdd(&results[cur_job], acc);
 }
 
 template <int G, bool STATS>
@@ -569,6 +636,90 @@ cudaError_t build_hub_bitmaps(const int64_t *off, const int32_t *adj,
 }
 
 size_t tile_smem_bytes() { return sizeof(TileSmem); }
+
+size_t batch_job_bytes() { return sizeof(BatchJob); }
+
+void batch_fill_job(void *dst, const GatPlan *d_plan, const GatPlan &h_plan,
+                    const DevGraphView &g, int linear_below, bool use_bitmaps) {
+    BatchJob j{};
+    SearchArgs &a = j.args;
+    a.plan = d_plan;
+    a.off = g.off;
+    a.adj = g.adj;
+    a.lo_off = g.lo_off;
+    a.V = g.V;
+    a.cap = g.max_degree > 0 ? g.max_degree : 1;
+    a.task_begin = 0;
+    a.num_tasks = h_plan.level1_bounded ? g.lo_total : g.E;
+    a.linear_below = linear_below;
+    const bool hubs = use_bitmaps && g.bitmaps != nullptr && g.hub_slot != nullptr;
+    a.hub_slot = hubs ? g.hub_slot : nullptr;
+    a.bitmaps = hubs ? g.bitmaps : nullptr;
+    a.bitmap_words = hubs ? g.bitmap_words : 0;
+    std::memcpy(dst, &j, sizeof(j));
+}
+
+int64_t batch_job_tasks(const void *job) {
+    return reinterpret_cast<const BatchJob *>(job)->args.num_tasks;
+}
+
+namespace {
+template <int G>
+cudaError_t batch_launch_g(const BatchJob *jobs, const int64_t *vstart, int32_t num_jobs,
+                           int64_t vtotal, int grid, int block, int chunk,
+                           unsigned long long *cursor, unsigned long long *results,
+                           int32_t *scratch, int64_t stride, cudaStream_t st) {
+    // The shared-memory attribute is set by batch_blocks_per_sm, which callers
+    // run first (outside any stream capture).
+    const size_t smem = size_t(block / G) * sizeof(TileSmem);
+    batch_kernel<G><<<grid, block, smem, st>>>(jobs, vstart, num_jobs, vtotal, chunk, cursor,
+                                               results, scratch, stride);
+    return cudaGetLastError();
+}
+template <int G>
+int batch_occ(int block) {
+    int n = 0;
+    const size_t smem = size_t(block / G) * sizeof(TileSmem);
+    cudaFuncSetAttribute(batch_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<G>, block, smem) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+}  // namespace
+
+int batch_blocks_per_sm(int tile, int block) {
+    switch (tile) {
+        case 1: return batch_occ<1>(block);
+        case 2: return batch_occ<2>(block);
+        case 4: return batch_occ<4>(block);
+        case 8: return batch_occ<8>(block);
+        case 16: return batch_occ<16>(block);
+        case 32: return batch_occ<32>(block);
+        default: return 0;
+    }
+}
+
+cudaError_t launch_batch(const void *d_jobs, const int64_t *d_vstart, int32_t num_jobs,
+                         int64_t vtotal, int tile, int grid, int block, int chunk,
+                         unsigned long long *d_cursor, unsigned long long *d_results,
+                         int32_t *scratch, int64_t stride, cudaStream_t st) {
+    const BatchJob *jobs = reinterpret_cast<const BatchJob *>(d_jobs);
+#define GAT_BL(G)                                                                        \
+    return batch_launch_g<G>(jobs, d_vstart, num_jobs, vtotal, grid, block, chunk, d_cursor, \
+                             d_results, scratch, stride, st)
+    switch (tile) {
+        case 1: GAT_BL(1);
+        case 2: GAT_BL(2);
+        case 4: GAT_BL(4);
+        case 8: GAT_BL(8);
+        case 16: GAT_BL(16);
+        case 32: GAT_BL(32);
+        default: return cudaErrorInvalidValue;
+    }
+#undef GAT_BL
+}
 
 int blocks_per_sm(int tile, int block, bool stats) {
 #define GAT_OCC(G) \

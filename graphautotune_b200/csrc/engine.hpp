@@ -43,6 +43,21 @@ struct LaunchShape {
     bool use_bitmaps = true; // use the graph's hub bitmaps when present
 };
 
+// Batched launches: host code fills an array of batch_job_bytes()-sized job
+// records (one per (plan, graph) pair), copies it and the chunk-aligned
+// virtual start of every job to the device, and launches one persistent
+// kernel over all of them.  `results` receives one signed 64-bit raw total
+// per job; cursor and results must be zero before the launch.
+size_t batch_job_bytes();
+void batch_fill_job(void *dst, const GatPlan *d_plan, const GatPlan &h_plan,
+                    const DevGraphView &g, int linear_below, bool use_bitmaps);
+int64_t batch_job_tasks(const void *job);
+int batch_blocks_per_sm(int tile, int block);
+cudaError_t launch_batch(const void *d_jobs, const int64_t *d_vstart, int32_t num_jobs,
+                         int64_t vtotal, int tile, int grid, int block, int chunk,
+                         unsigned long long *d_cursor, unsigned long long *d_results,
+                         int32_t *scratch, int64_t stride, cudaStream_t st);
+
 // Counts `plan` on a caller-owned device CSR without allocating: counters,
 // plan and per-tile set scratch live in the library's static device array
 // (GAT_NOALLOC_SCRATCH_BYTES, include/gat.h).  Writes the count (raw sum /

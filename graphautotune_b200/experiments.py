@@ -1,0 +1,176 @@
+"""Drivers for the benchmark configurations other than bench.py's headline
+(R-MAT 2^20, 4-clique + 4-cycle).  Each prints JSON lines.
+
+    python -m graphautotune_b200.experiments c1      # ER 10^4 triangle: exact, ref, timing
+    python -m graphautotune_b200.experiments c3      # R-MAT 2^22 house + 5-clique
+    python -m graphautotune_b200.experiments c4 [--tune N]
+                                                     # 21 patterns x 64 graphs: plain
+                                                     # launches vs one batched launch
+
+Graphs are synthetic and seeded (splitmix64 streams in libgat).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+
+import graphautotune_b200 as g
+
+TRIANGLE = "011101110"
+HOUSE_P2 = "0100110110010110110010100"
+K5 = "0111110111110111110111110"
+
+
+def emit(**kw):
+    print(json.dumps(kw), flush=True)
+
+
+def splitmix(x: int) -> int:
+    x = (x + 0x9E3779B97F4A7C15) & (2**64 - 1)
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & (2**64 - 1)
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & (2**64 - 1)
+    return z ^ (z >> 31)
+
+
+def c4_graph_spec(seed: int) -> dict:
+    """Configuration 4's graph for `seed` (100..163): n log-uniform in
+    [10^4, 10^6]; even seeds R-MAT with average degree 16 on 2^round(log2 n)
+    vertices (R-MAT needs a power of two), odd seeds Barabasi-Albert with m
+    drawn uniformly from 4..32."""
+    u = (splitmix(seed) >> 11) / float(1 << 53)
+    n = int(round(10 ** (4 + 2 * u)))
+    if seed % 2 == 0:
+        scale = max(1, int(round(math.log2(n))))
+        return {"seed": seed, "kind": "rmat", "scale": scale, "samples": 8 << scale}
+    m = 4 + (splitmix(seed ^ 0x5EED) % 29)
+    return {"seed": seed, "kind": "ba", "n": n, "m": int(m)}
+
+
+def make_graph(spec: dict) -> "g.Graph":
+    if spec["kind"] == "rmat":
+        return g.Graph.rmat(spec["scale"], spec["samples"], 0.57, 0.19, 0.19, spec["seed"])
+    return g.Graph.barabasi_albert(spec["n"], spec["m"], spec["seed"])
+
+
+def plain_config() -> "g.Config":
+    """The reference's generated default config (default_config.hpp:5)."""
+    return g.Config.reference_default()
+
+
+def run_c1(args):
+    gr = g.Graph.erdos_renyi(10000, 16.0, 1)
+    V, E, md = gr.info()
+    ex = g.Executor()
+    for mode in ("exact", "ref"):
+        s = g.Schedule(TRIANGLE, mode)
+        r = ex.count(gr, s)
+        times = [ex.count(gr, s).kernel_ms for _ in range(5)]
+        emit(config="c1", mode=mode, V=V, E=E, count=r.count, kernel_ms=min(times),
+             matches_per_s=(r.count if mode == "exact" else r.count / 3) / (min(times) / 1e3))
+
+
+def run_c3(args):
+    t0 = time.time()
+    gr = g.Graph.rmat(22, 1 << 26, 0.57, 0.19, 0.19, 3)
+    V, E, md = gr.info()
+    gr.upload(degree_order=True)
+    emit(config="c3", graph="R-MAT scale 22, 2^26 samples, seed 3", V=V, E=E, max_degree=md,
+         setup_s=time.time() - t0)
+    ex = g.Executor()
+    out = {}
+    for name, pat in (("house", HOUSE_P2), ("k5", K5)):
+        for mode in ("exact", "ref"):
+            s = g.Schedule(pat, mode)
+            # estimate from a slice before committing to the full count
+            raw, rs = ex.count_shard(gr, s, 0, 64)
+            est_s = rs.kernel_ms * 64 / 1e3
+            if est_s > args.max_seconds:
+                emit(config="c3", pattern=name, mode=mode, skipped=True,
+                     estimate_s=est_s)
+                continue
+            r = ex.count(gr, s)
+            out[(name, mode)] = r.count
+            emit(config="c3", pattern=name, mode=mode, count=r.count, kernel_ms=r.kernel_ms,
+                 matches_per_s=r.count / (r.kernel_ms / 1e3) if mode == "exact" else None)
+    if ("house", "exact") in out and ("house", "ref") in out:
+        emit(config="c3", check="ref house (P2 labelling) == exact house",
+             ok=out[("house", "exact")] == out[("house", "ref")])
+    if ("k5", "exact") in out and ("k5", "ref") in out:
+        emit(config="c3", check="ref 5-clique == 5 x exact", ok=out[("k5", "ref")] ==
+             5 * out[("k5", "exact")])
+
+
+def c4_jobs(graphs, patterns):
+    return [(gi, p) for gi in range(len(graphs)) for p in patterns]
+
+
+def run_c4(args):
+    seeds = list(range(100, 100 + args.graphs))
+    t0 = time.time()
+    specs = [c4_graph_spec(s) for s in seeds]
+    graphs = [make_graph(sp) for sp in specs]
+    for gr in graphs:
+        gr.upload(degree_order=True)
+    pats = g.enumerate_patterns(5)
+    scheds = {p: g.Schedule(p, "exact") for p in pats}
+    tot_e = sum(gr.info()[1] for gr in graphs)
+    emit(config="c4", graphs=len(graphs), patterns=len(pats), total_directed_edges=tot_e,
+         setup_s=time.time() - t0, specs=specs)
+    # plain: one default-config launch per job, each synchronised
+    ex = g.Executor(plain_config())
+    plain_counts, plain_ms, plain_wall = [], 0.0, 0.0
+    t = time.perf_counter()
+    for gr in graphs:
+        for p in pats:
+            r = ex.count(gr, scheds[p])
+            plain_counts.append(r.count)
+            plain_ms += r.kernel_ms
+    plain_wall = (time.perf_counter() - t) * 1e3
+    emit(config="c4", arm="plain", launches=len(plain_counts), kernel_ms=plain_ms,
+         wall_ms=plain_wall)
+    # batched: one persistent launch over all jobs, CUDA graph replay
+    b = g.Batch()
+    for gr in graphs:
+        for p in pats:
+            b.add(gr, scheds[p])
+    cfg = g.Config.engine_default()
+    if args.tune:
+        from graphautotune_b200 import tuner
+
+        cfg, hist = tuner.tune_batch(b, budget=args.tune)
+        emit(config="c4", arm="tuner", history=hist)
+    b.prepare(cfg, cuda_graph=True)
+    b.run()
+    runs = []
+    for _ in range(3):
+        t = time.perf_counter()
+        r = b.run()
+        runs.append(((time.perf_counter() - t) * 1e3, r.kernel_ms))
+    counts = b.counts()
+    assert counts == plain_counts, "batched counts differ from the plain launches"
+    best_wall = min(x[0] for x in runs)
+    emit(config="c4", arm="batched", launches=1, kernel_ms=min(x[1] for x in runs),
+         wall_ms=best_wall, config_used={k: getattr(cfg, k) for k in cfg._FIELDS},
+         speedup_vs_plain_wall=plain_wall / best_wall, counts_equal=True,
+         matches=sum(counts))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("config", choices=["c1", "c3", "c4"])
+    ap.add_argument("--graphs", type=int, default=64)
+    ap.add_argument("--tune", type=int, default=0)
+    ap.add_argument("--max-seconds", type=float, default=120.0)
+    args = ap.parse_args()
+    import torch
+
+    torch.cuda.set_device(0)
+    {"c1": run_c1, "c3": run_c3, "c4": run_c4}[args.config](args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -228,6 +228,26 @@ int gat_executor_count_shard(gat_executor *e, gat_graph *g,
                              const gat_schedule *s, void *stream,
                              int32_t shard, int32_t num_shards,
                              int64_t *raw_sum, gat_stats *stats);
+/* ---------------------------------------------------------------- batch --
+ * No single reference counterpart: the reference runs one pm process per
+ * (pattern, graph, config) (tuning/tuning/role/driver.py:88-132).  A batch
+ * counts many (schedule, graph) jobs of uneven size in ONE persistent launch:
+ * the jobs' level-1 work queues are concatenated (each rounded up to a whole
+ * chunk) and drained by one atomic cursor, so small jobs do not leave the GPU
+ * idle.  gat_batch_prepare fixes the launch shape from `c`, uploads graphs
+ * that are not resident yet, builds the job table and, with use_cuda_graph,
+ * captures memset + launch + result copy into a CUDA graph that
+ * gat_batch_run replays.  Counts follow each schedule's mode. */
+typedef struct gat_batch gat_batch;
+int gat_batch_create(gat_batch **out);
+int gat_batch_add(gat_batch *b, gat_graph *g, const gat_schedule *s,
+                  int32_t *job_index);
+int gat_batch_prepare(gat_batch *b, const gat_config *c, int use_cuda_graph);
+int gat_batch_run(gat_batch *b, gat_stats *stats);
+int gat_batch_counts(const gat_batch *b, uint64_t *counts, size_t n);
+int gat_batch_size(const gat_batch *b);
+void gat_batch_free(gat_batch *b);
+
 /* ------------------------------------------------------ allocation-free --
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory when they count: a host framework whose caching allocator already

@@ -65,8 +65,12 @@ GRAPHS = {
     "ba60": ("ba", (60, 3), 14),
     "k5": ("complete", (5,), 0),
     "k7": ("complete", (7,), 0),
+    # configuration 1 at full size: G(n=10,000, avg degree 16), seed 1
+    "c1_er10000": ("er", (10000, 16.0), 1),
 }
-NAIVE_TIMEOUT_S = 60
+# Full-size graphs get only the configuration's own pattern.
+ONLY = {"c1_er10000": {"triangle"}}
+NAIVE_TIMEOUT_S = 600
 
 
 def connected_order(p: str) -> str:
@@ -196,6 +200,10 @@ def main() -> None:
     for gname, gpath in graphs.items():
         for pname, p in pats:
             n = int(round(len(p) ** 0.5))
+            if gname in ONLY:
+                if pname in ONLY[gname]:
+                    jobs.append((gname, pname, gpath, p))
+                continue
             if n >= 6 and gname not in ("er60", "k7", "k5"):
                 continue
             if n >= 5 and gname == "er200":

@@ -130,10 +130,12 @@ class Config:
     chunk: int = 16
     hub_bitmaps: int = 1
     memory_budget: int = 0
+    special_kernels: int = 1
 
     _FIELDS = ("set_search_type", "set_intersection_type", "vertex_store_type",
                "graph_backend_type", "num_blocks", "threads_per_block",
-               "threads_per_warp", "max_regs", "chunk", "hub_bitmaps", "memory_budget")
+               "threads_per_warp", "max_regs", "chunk", "hub_bitmaps", "memory_budget",
+               "special_kernels")
 
     @classmethod
     def _from_c(cls, c: gat_config) -> "Config":

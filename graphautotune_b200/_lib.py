@@ -50,7 +50,9 @@ class gat_config(C.Structure):
         ("chunk", C.c_int32),
         ("hub_bitmaps", C.c_int32),
         ("memory_budget", C.c_int64),
-        ("reserved", C.c_int64 * 4),
+        ("special_kernels", C.c_int32),
+        ("reserved1", C.c_int32),
+        ("reserved", C.c_int64 * 3),
     ]
 
 

@@ -1,0 +1,321 @@
+"""Learned cost model for schedule/configuration choice.
+
+A 3-layer FP32 perceptron (libgat's gat_mlp_*: hand-written forward,
+backward and Adam kernels) maps features of (plan, launch configuration,
+data graph) to log run time.  It is trained on timings the engine itself
+records (`collect`), and used to rank candidate configurations (`pick`),
+replacing the reference tuner's XGBoost model over configuration indices
+(tuning/tuning/role/modeling.py:81-102); the measured-search tuner
+(graphautotune_b200.tuner) is its fallback and the judge of its ranking.
+
+    python -m graphautotune_b200.costmodel collect --runs 20000 --out data.npz
+    python -m graphautotune_b200.costmodel train data.npz --out model.npz
+    python -m graphautotune_b200.costmodel eval5 --model model.npz
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import random
+import sys
+import time
+
+import numpy as np
+
+import graphautotune_b200 as g
+from graphautotune_b200 import tuner
+from graphautotune_b200._lib import check, lib
+
+HIST_BUCKETS = 15
+N_FEATURES = 7 + 10 + 5 + HIST_BUCKETS
+
+
+def _bind():
+    l = lib()
+    P = C.c_void_p
+    fp = C.POINTER(C.c_float)
+    sigs = {
+        "gat_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(P)]),
+        "gat_mlp_free": (None, [P]),
+        "gat_mlp_num_params": (C.c_int, [P]),
+        "gat_mlp_get_params": (C.c_int, [P, fp, C.c_int]),
+        "gat_mlp_set_params": (C.c_int, [P, fp, C.c_int]),
+        "gat_mlp_predict": (C.c_int, [P, fp, C.c_int, fp]),
+        "gat_mlp_gradient": (C.c_int, [P, fp, fp, C.c_int, fp, fp]),
+        "gat_mlp_train": (C.c_int, [P, fp, fp, C.c_int, C.c_int, C.c_int, C.c_float,
+                                    C.c_uint64, fp]),
+        "gat_mlp_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(l, name)
+        f.restype, f.argtypes = res, args
+    return l
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _check_mlp(rc: int) -> None:
+    if rc != 0:
+        raise g.GatError(rc, lib().gat_mlp_last_error().decode())
+
+
+class MLP:
+    """gat_mlp handle: in -> 64 -> 64 -> 1."""
+
+    def __init__(self, in_features: int = N_FEATURES, seed: int = 0):
+        self.l = _bind()
+        self.h = C.c_void_p()
+        self.in_features = in_features
+        _check_mlp(self.l.gat_mlp_create(in_features, seed, C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.l.gat_mlp_free(self.h)
+
+    @property
+    def num_params(self) -> int:
+        return self.l.gat_mlp_num_params(self.h)
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.num_params, np.float32)
+        _check_mlp(self.l.gat_mlp_get_params(self.h, _fp(out), len(out)))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        _check_mlp(self.l.gat_mlp_set_params(self.h, _fp(p), len(p)))
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.zeros(len(X), np.float32)
+        _check_mlp(self.l.gat_mlp_predict(self.h, _fp(X), len(X), _fp(y)))
+        return y
+
+    def gradient(self, X: np.ndarray, T: np.ndarray) -> tuple[np.ndarray, float]:
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        grad = np.zeros(self.num_params, np.float32)
+        loss = C.c_float()
+        _check_mlp(self.l.gat_mlp_gradient(self.h, _fp(X), _fp(T), len(X), _fp(grad),
+                                           C.byref(loss)))
+        return grad, loss.value
+
+    def train(self, X: np.ndarray, T: np.ndarray, epochs: int = 200, batch: int = 256,
+              lr: float = 1e-3, seed: int = 0) -> float:
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        loss = C.c_float()
+        _check_mlp(self.l.gat_mlp_train(self.h, _fp(X), _fp(T), len(X), epochs, batch, lr,
+                                        seed, C.byref(loss)))
+        return loss.value
+
+
+# ------------------------------------------------------------------ features
+
+def graph_features(graph: "g.Graph") -> np.ndarray:
+    off, _ = graph.csr()
+    deg = np.diff(off)
+    V = max(len(deg), 1)
+    E = int(off[-1])
+    md = int(deg.max()) if len(deg) else 0
+    hist = np.zeros(HIST_BUCKETS, np.float32)
+    nz = deg[deg > 0]
+    if len(nz):
+        b = np.minimum(np.floor(np.log2(nz)).astype(int), HIST_BUCKETS - 1)
+        hist += np.bincount(b, minlength=HIST_BUCKETS)[:HIST_BUCKETS] / V
+    hub = float(deg[deg >= 512].sum()) / max(E, 1)
+    return np.concatenate([[math.log10(V) / 7, math.log10(max(E, 1)) / 9,
+                            math.log10(max(md, 1)) / 6, (E / V) / 64, hub], hist]).astype(
+        np.float32)
+
+
+def plan_features(sched: "g.Schedule") -> np.ndarray:
+    raw = sched.plan_bytes()
+    i32 = np.frombuffer(raw[:40], np.int32)
+    n, basic, num_prefix, mode, collide, l1b, num_store, iep_num, num_terms = i32[:9]
+    divisor = np.frombuffer(raw[40:48], np.int64)[0]
+    kinds = np.frombuffer(raw[48 + 64:48 + 96], np.int8)[:num_prefix]
+    edges = sched.pattern.adjacency().count("1") // 2
+    return np.array([n / 10, basic / 10, num_prefix / 16, num_store / 8, iep_num / 8,
+                     num_terms / 16, math.log2(max(int(divisor), 1)) / 10, float(l1b),
+                     float((kinds == 2).sum()) / 8, edges / 45], np.float32)
+
+
+def config_features(d: dict) -> np.ndarray:
+    s = d["vertex_set_config.set_search_type"]
+    nb = d["engine_config.launch_config.num_blocks"]
+    return np.array([math.log2(s + 1) / 31, float(nb == 0), math.log2(nb + 1) / 11,
+                     math.log2(d["engine_config.launch_config.threads_per_block"]) / 8,
+                     math.log2(d["engine_config.launch_config.threads_per_warp"]) / 5,
+                     math.log2(d["engine_config.chunk"]) / 6,
+                     float(d["engine_config.hub_bitmaps"])], np.float32)
+
+
+def features(gf: np.ndarray, pf: np.ndarray, d: dict) -> np.ndarray:
+    return np.concatenate([config_features(d), pf, gf]).astype(np.float32)
+
+
+# ---------------------------------------------------------------- data
+
+def training_graphs(count: int, seed0: int = 1000) -> list[dict]:
+    """Graphs like configuration 4's, smaller: n log-uniform in [2^10, 2^16],
+    half R-MAT (average degree 16), half Barabasi-Albert (m in 4..32)."""
+    from graphautotune_b200.experiments import splitmix
+
+    specs = []
+    for i in range(count):
+        s = seed0 + i
+        u = (splitmix(s) >> 11) / float(1 << 53)
+        n = int(2 ** (10 + 6 * u))
+        if i % 2 == 0:
+            scale = max(1, int(round(math.log2(n))))
+            specs.append({"seed": s, "kind": "rmat", "scale": scale, "samples": 8 << scale})
+        else:
+            specs.append({"seed": s, "kind": "ba", "n": n, "m": 4 + splitmix(s ^ 7) % 29})
+    return specs
+
+
+def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
+            log=None) -> tuple[np.ndarray, np.ndarray]:
+    """Times `runs` random (graph, pattern, configuration) counts."""
+    from graphautotune_b200.experiments import make_graph
+
+    rng = random.Random(seed)
+    pats = g.enumerate_patterns(4) + g.enumerate_patterns(5)
+    glist = []
+    for sp in training_graphs(graphs):
+        gr = make_graph(sp)
+        gr.upload(degree_order=True)
+        glist.append((gr, graph_features(gr)))
+    scheds = [g.Schedule(p, "exact") for p in pats]
+    pfs = [plan_features(s) for s in scheds]
+    X, T = [], []
+    execs: dict[str, g.Executor] = {}
+    slow: set = set()
+    t0 = time.time()
+    while len(X) < runs:
+        gi, si = rng.randrange(len(glist)), rng.randrange(len(scheds))
+        if (gi, si) in slow:
+            continue
+        d = tuner.random_point(rng)
+        key = tuner.fingerprint(d)
+        if key not in execs:
+            execs[key] = g.Executor(tuner.to_config(d))
+        gr, gf = glist[gi]
+        r = execs[key].count(gr, scheds[si])
+        if r.kernel_ms > max_ms:
+            slow.add((gi, si))  # keep the data set cheap to gather
+        X.append(features(gf, pfs[si], d))
+        T.append(math.log(max(r.kernel_ms, 1e-3)))
+        if log and len(X) % 1000 == 0:
+            log(f"collected {len(X)} runs in {time.time() - t0:.1f}s")
+    return np.stack(X), np.array(T, np.float32)
+
+
+class CostModel:
+    def __init__(self, mlp: MLP, mean: np.ndarray, std: np.ndarray):
+        self.mlp, self.mean, self.std = mlp, mean, std
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        return self.mlp.predict((X - self.mean) / self.std)
+
+    def save(self, path: str) -> None:
+        np.savez(path, params=self.mlp.params(), mean=self.mean, std=self.std)
+
+    @classmethod
+    def load(cls, path: str) -> "CostModel":
+        z = np.load(path)
+        m = MLP(len(z["mean"]))
+        m.set_params(z["params"])
+        return cls(m, z["mean"], z["std"])
+
+    @classmethod
+    def fit(cls, X: np.ndarray, T: np.ndarray, epochs: int = 200, seed: int = 0,
+            lr: float = 1e-3) -> tuple["CostModel", float]:
+        mean = X.mean(0)
+        std = X.std(0) + 1e-6
+        m = MLP(X.shape[1], seed)
+        loss = m.train((X - mean) / std, T, epochs=epochs, lr=lr, seed=seed)
+        return cls(m, mean, std), loss
+
+
+class TunerModel:
+    """Adapter so the tuner's simulated annealing ranks points with the MLP."""
+
+    def __init__(self, model: CostModel, gf: np.ndarray, pf: np.ndarray):
+        self.model, self.gf, self.pf = model, gf, pf
+
+    def predict(self, xs: list[dict]) -> list[float]:
+        X = np.stack([features(self.gf, self.pf, d) for d in xs])
+        return self.model.predict(X).tolist()
+
+
+def all_points() -> list[dict]:
+    import itertools
+
+    keys = tuner.KEYS
+    out = []
+    for vals in itertools.product(*(tuner.SPACE[k] for k in keys)):
+        d = dict(zip(keys, vals))
+        if tuner.valid(d):
+            out.append(d)
+    return out
+
+
+def pick(model: CostModel, gf: np.ndarray, pf: np.ndarray, points: list[dict]) -> dict:
+    X = np.stack([features(gf, pf, d) for d in points])
+    return points[int(np.argmin(model.predict(X)))]
+
+
+# ---------------------------------------------------------------- CLI
+
+def main():
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    c = sub.add_parser("collect")
+    c.add_argument("--runs", type=int, default=20000)
+    c.add_argument("--out", default="costmodel_data.npz")
+    c.add_argument("--seed", type=int, default=0)
+    t = sub.add_parser("train")
+    t.add_argument("data")
+    t.add_argument("--out", default="costmodel.npz")
+    t.add_argument("--epochs", type=int, default=200)
+    e = sub.add_parser("eval5")
+    e.add_argument("--model", required=True)
+    e.add_argument("--parts", type=int, default=256)
+    e.add_argument("--candidates", type=int, default=48)
+    a = ap.parse_args()
+    import torch
+
+    torch.cuda.set_device(0)
+    if a.cmd == "collect":
+        X, T = collect(a.runs, a.seed, log=lambda s: print(s, file=sys.stderr, flush=True))
+        np.savez(a.out, X=X, T=T)
+        print(json.dumps({"runs": len(X), "features": X.shape[1], "out": a.out}))
+    elif a.cmd == "train":
+        z = np.load(a.data)
+        X, T = z["X"], z["T"]
+        idx = np.random.default_rng(0).permutation(len(X))
+        cut = int(0.9 * len(X))
+        tr, te = idx[:cut], idx[cut:]
+        t0 = time.time()
+        model, loss = CostModel.fit(X[tr], T[tr], epochs=a.epochs)
+        pred = model.predict(X[te])
+        test_mse = float(np.mean((pred - T[te]) ** 2))
+        base_mse = float(np.mean((T[tr].mean() - T[te]) ** 2))
+        model.save(a.out)
+        print(json.dumps({"train_mse": loss, "test_mse": test_mse,
+                          "test_mse_predicting_mean": base_mse, "seconds": time.time() - t0,
+                          "out": a.out}))
+    elif a.cmd == "eval5":
+        from graphautotune_b200.experiments import eval_c5
+
+        eval_c5(CostModel.load(a.model), parts=a.parts, n_candidates=a.candidates)
+
+
+if __name__ == "__main__":
+    main()

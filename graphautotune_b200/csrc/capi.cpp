@@ -106,6 +106,7 @@ struct gat_executor {
     int sms = 0;
     int32_t *scratch = nullptr;
     size_t scratch_bytes = 0;
+    bool scratch_clean = false;  // all-zero (the 4-cycle kernel's invariant)
     DevCounters *ctr = nullptr;
     DevCounters *host_ctr = nullptr;  // pinned
     GatPlan *d_plan = nullptr;
@@ -256,6 +257,7 @@ void gat_config_default(gat_config *c) {
     c->max_regs = 32;
     c->chunk = 16;
     c->hub_bitmaps = 1;
+    c->special_kernels = 1;
     c->memory_budget = 0;
 }
 
@@ -310,6 +312,7 @@ bool set_field(gat_config *c, const std::string &key, const std::string &val) {
     if (k == "max_regs") return i32(c->max_regs);
     if (k == "chunk") return i32(c->chunk);
     if (k == "hub_bitmaps") return i32(c->hub_bitmaps);
+    if (k == "special_kernels") return i32(c->special_kernels);
     if (k == "memory_budget") {
         c->memory_budget = x;
         return true;
@@ -620,6 +623,71 @@ void gat_executor_free(gat_executor *e) { delete e; }
 
 namespace {
 
+// The exact 4-cycle count through the wedge-aggregation kernel: one V-word
+// counter row per resident tile, kept all-zero between launches.
+int run_c4(gat_executor *e, const DevGraphView &view, int64_t vb, int64_t ve,
+           LaunchShape shape, cudaStream_t strm, bool balg, bool ranged, uint64_t *count,
+           gat_stats *stats, std::chrono::steady_clock::time_point t0) {
+    const int occ = c4_blocks_per_sm(shape.tile, shape.block, balg);
+    if (occ <= 0) return fail(GAT_ERR_CUDA, "4-cycle kernel does not fit on the device");
+    shape.grid = e->cfg.num_blocks > 0 ? e->cfg.num_blocks : e->sms * occ;
+    const int64_t stride = std::max<int64_t>(view.V, 1);
+    const int64_t per_block = int64_t(shape.block / shape.tile) * stride * 4;
+    const int64_t budget = e->cfg.memory_budget > 0 ? e->cfg.memory_budget : (int64_t(16) << 30);
+    if (per_block > budget) return fail(GAT_ERR_MEMORY, "memory budget below one CTA's counters");
+    shape.grid = (int)std::min<int64_t>(shape.grid, budget / per_block);
+    const size_t need = size_t(per_block) * size_t(shape.grid);
+    cudaError_t ce;
+    if (need > e->scratch_bytes) {
+        cudaFree(e->scratch);
+        e->scratch = nullptr;
+        e->scratch_bytes = 0;
+        if ((ce = cudaMalloc(&e->scratch, need)) != cudaSuccess)
+            return fail(GAT_ERR_MEMORY, std::string("counter allocation: ") + cudaGetErrorString(ce));
+        e->scratch_bytes = need;
+        e->scratch_clean = false;
+    }
+    if (!e->scratch_clean) {
+        if ((ce = cudaMemsetAsync(e->scratch, 0, e->scratch_bytes, strm)) != cudaSuccess)
+            return cuda_fail(ce, "counter clear");
+        e->scratch_clean = true;
+    }
+    cudaEventRecord(e->ev0, strm);
+    ce = launch_c4(view, vb, ve, shape.tile, shape.grid, shape.block, shape.chunk, e->ctr,
+                   reinterpret_cast<uint32_t *>(e->scratch), stride, balg, strm);
+    if (ce != cudaSuccess) {
+        e->scratch_clean = false;
+        return cuda_fail(ce, "4-cycle launch");
+    }
+    cudaEventRecord(e->ev1, strm);
+    if ((ce = cudaMemcpyAsync(e->host_ctr, e->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                              strm)) != cudaSuccess ||
+        (ce = cudaStreamSynchronize(strm)) != cudaSuccess) {
+        e->scratch_clean = false;
+        return cuda_fail(ce, "4-cycle count");
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    const int64_t raw = (int64_t)e->host_ctr->result;
+    *count = (uint64_t)raw;
+    gat_stats st{};
+    st.kernel_ms = ms;
+    st.raw_sum = raw;
+    st.divisor = 1;
+    st.tasks = (uint64_t)(ve - vb);
+    st.balg_bytes = e->host_ctr->bytes;
+    st.grid = shape.grid;
+    st.block = shape.block;
+    st.tile = shape.tile;
+    st.launches = 1;
+    st.scratch_bytes = (int64_t)need;
+    st.total_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    (void)ranged;
+    if (stats) *stats = st;
+    return GAT_OK;
+}
+
 int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *stream,
                uint64_t *count, gat_stats *stats, bool balg, int64_t root_begin = -1,
                int64_t root_end = -1, int shard = 0, int num_shards = 0) {
@@ -686,9 +754,28 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
         shape.task_begin = toff[root_begin];
         shape.task_end = toff[root_end];
     }
+    if (plan.special == GAT_SPECIAL_C4 && s->mode == GAT_MODE_EXACT &&
+        e->cfg.special_kernels != 0) {
+        // First-vertex range of this call: whole graph, a root range, or the
+        // vertices whose level-1 units start inside the shard's unit range.
+        int64_t vb = 0, ve = view.V;
+        if (root_begin >= 0) {
+            vb = root_begin;
+            ve = root_end;
+        } else if (num_shards > 0) {
+            const auto &lo = dc->lo_host;
+            vb = std::lower_bound(lo.begin(), lo.begin() + view.V, shape.task_begin) - lo.begin();
+            ve = shard + 1 == num_shards
+                     ? view.V
+                     : std::lower_bound(lo.begin(), lo.begin() + view.V, shape.task_end) -
+                           lo.begin();
+        }
+        return run_c4(e, view, vb, ve, shape, strm, balg, ranged, count, stats, t0);
+    }
     int occ = blocks_per_sm(shape.tile, shape.block, balg);
     if (occ <= 0) return fail(GAT_ERR_CUDA, "kernel does not fit on the device");
     shape.grid = e->cfg.num_blocks > 0 ? e->cfg.num_blocks : e->sms * occ;
+    e->scratch_clean = false;
     const int64_t stride = tile_scratch_ints(plan, view.max_degree);
     const int64_t tiles_per_block = shape.block / shape.tile;
     const int64_t budget = e->cfg.memory_budget > 0 ? e->cfg.memory_budget : (int64_t(4) << 30);

@@ -567,6 +567,69 @@ __global__ void __launch_bounds__(256)
     if (t.lane == 0 && cur_job >= 0 && acc) atomicAdd(&results[cur_job], acc);
 }
 
+// Exact 4-cycle count by wedge aggregation.  Every 4-cycle is counted once,
+// at its largest vertex v0 together with the vertex x opposite v0: its other
+// two vertices are common neighbours of v0 and x below v0.  So
+//   count = sum_{v0} sum_{x < v0} C(c(v0, x), 2),
+//   c(v0, x) = |{ v1 in N(v0) : v1 < v0, x in N(v1) }|   (x < v0 too).
+// A tile owns a range of v0 and a private counter row of V words in scratch
+// (all zero between vertices): pass 1 adds 1 to cnt[x] for every wedge
+// v0 - v1 - x with v1, x < v0; pass 2 walks the same wedges and takes each
+// counter with an atomic exchange against 0, so every x contributes its
+// C(c, 2) exactly once and the row is zero again afterwards.  The lower
+// neighbours of v0 are the prefix of its sorted row (lo_off), and each N(v1)
+// is cut at v0 by a lower bound.
+template <int G, bool STATS>
+__global__ void __launch_bounds__(256)
+    c4_wedge_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                    const int64_t *__restrict__ lo_off, int64_t v_begin, int64_t v_end,
+                    int32_t chunk, DevCounters *ctr, uint32_t *cnt_all, int64_t cnt_stride) {
+    const Tile<G> t;
+    const int tiles_per_block = blockDim.x / G;
+    const int tile_in_block = threadIdx.x / G;
+    uint32_t *cnt =
+        cnt_all + ((int64_t)blockIdx.x * tiles_per_block + tile_in_block) * cnt_stride;
+    unsigned long long part = 0, bytes = 0;
+    for (;;) {
+        unsigned long long s = 0;
+        if (t.lane == 0)
+            s = (unsigned long long)v_begin + atomicAdd(&ctr->cursor, (unsigned long long)chunk);
+        s = t.bcast(s, 0);
+        if (s >= (unsigned long long)v_end) break;
+        const int64_t e = min((int64_t)s + chunk, v_end);
+        for (int64_t v0 = (int64_t)s; v0 < e; v0++) {
+            const int32_t nlo = (int32_t)(lo_off[v0 + 1] - lo_off[v0]);
+            if (nlo < 2) continue;
+            const int32_t *l0 = adj + off[v0];
+            for (int i = 0; i < nlo; i++) {
+                const int32_t v1 = l0[i];
+                const int64_t o1 = off[v1];
+                const int n1 = tile_bound<G, false>(t, adj + o1, (int)(off[v1 + 1] - o1),
+                                                    (int32_t)v0);
+                for (int k = t.lane; k < n1; k += G) atomicAdd(&cnt[adj[o1 + k]], 1u);
+                if (STATS && t.lane == 0) bytes += 8ull * (unsigned)n1;
+            }
+            t.sync();
+            for (int i = 0; i < nlo; i++) {
+                const int32_t v1 = l0[i];
+                const int64_t o1 = off[v1];
+                const int n1 = tile_bound<G, false>(t, adj + o1, (int)(off[v1 + 1] - o1),
+                                                    (int32_t)v0);
+                for (int k = t.lane; k < n1; k += G) {
+                    const unsigned long long c = atomicExch(&cnt[adj[o1 + k]], 0u);
+                    part += c * (c - 1) / 2;
+                }
+            }
+            t.sync();
+        }
+    }
+    part = t.sum(part);
+    if (t.lane == 0) {
+        atomicAdd(&ctr->result, part);
+        if (STATS) atomicAdd(&ctr->bytes, bytes);
+    }
+}
+
 template <int G, bool STATS>
 cudaError_t launch_one(const SearchArgs &a, int grid, int block,
                        cudaStream_t stream) {
@@ -688,6 +751,58 @@ int batch_occ(int block) {
     return n;
 }
 }  // namespace
+
+namespace {
+template <int G, bool STATS>
+int c4_occ(int block) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, c4_wedge_kernel<G, STATS>, block, 0) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+}  // namespace
+
+int c4_blocks_per_sm(int tile, int block, bool stats) {
+#define GAT_C4O(G) return stats ? c4_occ<G, true>(block) : c4_occ<G, false>(block)
+    switch (tile) {
+        case 1: GAT_C4O(1);
+        case 2: GAT_C4O(2);
+        case 4: GAT_C4O(4);
+        case 8: GAT_C4O(8);
+        case 16: GAT_C4O(16);
+        case 32: GAT_C4O(32);
+        default: return 0;
+    }
+#undef GAT_C4O
+}
+
+cudaError_t launch_c4(const DevGraphView &g, int64_t v_begin, int64_t v_end, int tile,
+                      int grid, int block, int chunk, DevCounters *ctr, uint32_t *cnt,
+                      int64_t stride, bool stats, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(DevCounters), st);
+    if (e != cudaSuccess) return e;
+    const int ch = chunk > 0 ? chunk : 1;
+#define GAT_C4L(G)                                                                             \
+    if (stats)                                                                                 \
+        c4_wedge_kernel<G, true><<<grid, block, 0, st>>>(g.off, g.adj, g.lo_off, v_begin,      \
+                                                         v_end, ch, ctr, cnt, stride);         \
+    else                                                                                       \
+        c4_wedge_kernel<G, false><<<grid, block, 0, st>>>(g.off, g.adj, g.lo_off, v_begin,     \
+                                                          v_end, ch, ctr, cnt, stride);        \
+    break
+    switch (tile) {
+        case 1: GAT_C4L(1);
+        case 2: GAT_C4L(2);
+        case 4: GAT_C4L(4);
+        case 8: GAT_C4L(8);
+        case 16: GAT_C4L(16);
+        case 32: GAT_C4L(32);
+        default: return cudaErrorInvalidValue;
+    }
+#undef GAT_C4L
+    return cudaGetLastError();
+}
 
 int batch_blocks_per_sm(int tile, int block) {
     switch (tile) {

@@ -43,6 +43,25 @@ struct LaunchShape {
     bool use_bitmaps = true; // use the graph's hub bitmaps when present
 };
 
+// Device counters used by one search: work-queue cursor, signed 64-bit
+// total (two's complement in an unsigned word), algorithmic bytes, error
+// flags.
+struct DevCounters {
+    unsigned long long cursor;
+    unsigned long long result;
+    unsigned long long bytes;
+    unsigned long long error;
+};
+
+// Exact 4-cycle count by wedge aggregation over first vertices
+// [v_begin, v_end) (plans with special == GAT_SPECIAL_C4).  `cnt` holds one
+// V-word counter row per resident tile (grid x block/tile rows of `stride`
+// words); rows must be zero before the launch and are zero again after it.
+int c4_blocks_per_sm(int tile, int block, bool stats);
+cudaError_t launch_c4(const DevGraphView &g, int64_t v_begin, int64_t v_end, int tile,
+                      int grid, int block, int chunk, DevCounters *ctr, uint32_t *cnt,
+                      int64_t stride, bool stats, cudaStream_t st);
+
 // Batched launches: host code fills an array of batch_job_bytes()-sized job
 // records (one per (plan, graph) pair), copies it and the chunk-aligned
 // virtual start of every job to the device, and launches one persistent
@@ -66,16 +85,6 @@ cudaError_t launch_batch(const void *d_jobs, const int64_t *d_vstart, int32_t nu
 int count_noalloc(const GatPlan &plan, const int64_t *d_off, const int32_t *d_adj,
                   int32_t V, int64_t E, int32_t max_degree, const LaunchShape &shape,
                   long long *d_count, cudaStream_t stream, std::string *err);
-
-// Device counters used by one search: work-queue cursor, signed 64-bit
-// total (two's complement in an unsigned word), algorithmic bytes, error
-// flags.
-struct DevCounters {
-    unsigned long long cursor;
-    unsigned long long result;
-    unsigned long long bytes;
-    unsigned long long error;
-};
 
 enum : unsigned long long {
     GAT_DEVERR_SCRATCH = 1ull,  // a stored set would overflow its slot

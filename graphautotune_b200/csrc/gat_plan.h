@@ -22,6 +22,8 @@
 #define GAT_MAX_PREFIX 32
 #define GAT_MAX_TERMS 64
 
+#define GAT_SPECIAL_C4 1
+
 enum {
     GAT_SET_ALIAS = 0,  /* N(v_level), truncated by p_trunc */
     GAT_SET_STORE = 1,  /* N(v_level) n father, materialised */
@@ -40,7 +42,9 @@ typedef struct GatPlan {
     int32_t num_store;     /* materialised prefixes = scratch slots per tile */
     int32_t iep_num;       /* IEP value slots */
     int32_t num_terms;     /* IEP subgroups */
-    int32_t pad0;
+    int32_t special;       /* 0: interpret this plan; GAT_SPECIAL_C4: the
+                              exact 4-cycle count has a dedicated kernel
+                              (the plan stays valid as its fallback) */
     int64_t divisor;       /* final count = sum / divisor */
 
     int8_t p_level[GAT_MAX_PREFIX];

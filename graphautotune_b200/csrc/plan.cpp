@@ -358,6 +358,13 @@ bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out,
     o << "exact plan: suffix " << best.k << ", divisor " << best.div
       << ", cost " << best.cost;
     out.summary = o.str();
+    // The 4-cycle (4 vertices, 4 edges, every degree 2) has a dedicated
+    // wedge-aggregation kernel; this plan remains its fallback.
+    if (p.n == 4 && p.edges() == 4) {
+        bool cyc = true;
+        for (int i = 0; i < 4; i++) cyc &= __builtin_popcount(p.row[i]) == 2;
+        if (cyc) pl.special = GAT_SPECIAL_C4;
+    }
     return true;
 }
 

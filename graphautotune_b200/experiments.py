@@ -17,6 +17,8 @@ import math
 import sys
 import time
 
+import numpy as np
+
 import graphautotune_b200 as g
 
 TRIANGLE = "011101110"
@@ -57,8 +59,9 @@ def make_graph(spec: dict) -> "g.Graph":
 
 
 def plain_config() -> "g.Config":
-    """The reference's generated default config (default_config.hpp:5)."""
-    return g.Config.reference_default()
+    """The engine's default configuration, as a user gets it without tuning
+    (one launch per (pattern, graph) job is the 'plain' arm)."""
+    return g.Config.engine_default()
 
 
 def run_c1(args):
@@ -157,6 +160,93 @@ def run_c4(args):
          wall_ms=best_wall, config_used={k: getattr(cfg, k) for k in cfg._FIELDS},
          speedup_vs_plain_wall=plain_wall / best_wall, counts_equal=True,
          matches=sum(counts))
+
+
+def _edges(n, pairs):
+    s = ["0"] * (n * n)
+    for u, v in pairs:
+        s[u * n + v] = s[v * n + u] = "1"
+    return "".join(s)
+
+
+C5_PATTERNS = {
+    "k6": _edges(6, [(i, j) for i in range(6) for j in range(i + 1, 6)]),
+    "c6_chord": _edges(6, [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5), (5, 0), (0, 3)]),
+    "tri_path_7v": _edges(7, [(0, 1), (1, 2), (0, 2), (2, 3), (3, 4), (4, 5), (5, 6)]),
+}
+
+
+def c5_candidates() -> list[dict]:
+    """The launch-shape sub-space measured exhaustively: tile x block x
+    chunk x hub bitmaps, binary search, persistent grid."""
+    from graphautotune_b200 import tuner
+
+    base = tuner.default_point()
+    out = []
+    for tile in (4, 8, 16, 32):
+        for block in (128, 256):
+            for chunk in (1, 4, 16, 64):
+                for hub in (0, 1):
+                    d = dict(base)
+                    d["engine_config.launch_config.threads_per_warp"] = tile
+                    d["engine_config.launch_config.threads_per_block"] = block
+                    d["engine_config.chunk"] = chunk
+                    d["engine_config.hub_bitmaps"] = hub
+                    out.append(d)
+    return out
+
+
+def eval_c5(model, parts: int = 256, n_candidates: int = 64):
+    """Configuration 5: the cost model picks a launch configuration for 6- and
+    7-vertex patterns on R-MAT 2^24 (average degree 24, seed 4); compared with
+    the default configuration and the best of the exhaustively measured
+    candidates.  Every measurement counts the same slice of the work queue
+    (shard 0 of `parts`) so that all configurations do identical work; counts
+    must agree across configurations."""
+    from graphautotune_b200 import costmodel, tuner
+
+    t0 = time.time()
+    gr = g.Graph.rmat(24, 12 << 24, 0.57, 0.19, 0.19, 4)
+    V, E, md = gr.info()
+    gr.upload(degree_order=True)
+    gf = costmodel.graph_features(gr)
+    emit(config="c5", graph="R-MAT scale 24, 12*2^24 samples (avg degree 24), seed 4", V=V,
+         E=E, max_degree=md, setup_s=time.time() - t0, slice=f"shard 0 of {parts}")
+    cands = c5_candidates()[:n_candidates]
+    for name, pat in C5_PATTERNS.items():
+        s = g.Schedule(pat, "exact", stats_graph=gr)
+        pf = costmodel.plan_features(s)
+
+        def measure(d):
+            ex = g.Executor(tuner.to_config(d))
+            raw, r = ex.count_shard(gr, s, 0, parts)
+            raw2, r2 = ex.count_shard(gr, s, 0, parts)
+            assert raw == raw2
+            return raw, min(r.kernel_ms, r2.kernel_ms)
+
+        default = tuner.default_point()
+        raw0, t_default = measure(default)
+        if t_default > 20000:
+            emit(config="c5", pattern=name, skipped="slice too slow", default_ms=t_default)
+            continue
+        picked = costmodel.pick(model, gf, pf, cands)
+        raw_p, t_pick = measure(picked)
+        times = []
+        for d in cands:
+            raw_c, t_c = measure(d)
+            assert raw_c == raw0, "counts differ across configurations"
+            times.append(t_c)
+        best = int(np.argmin(times))
+        pred = model.predict(np.stack([costmodel.features(gf, pf, d) for d in cands]))
+        rank_corr = float(np.corrcoef(np.argsort(np.argsort(pred)),
+                                      np.argsort(np.argsort(times)))[0, 1])
+        emit(config="c5", pattern=name, slice_raw_count=raw0, default_ms=t_default,
+             model_pick_ms=t_pick, best_measured_ms=times[best],
+             median_candidate_ms=float(np.median(times)),
+             pick_vs_default=t_default / t_pick, pick_vs_best=times[best] / t_pick,
+             spearman_pred_vs_measured=rank_corr, candidates=len(cands),
+             picked={k.split(".")[-1]: v for k, v in picked.items()},
+             best={k.split(".")[-1]: v for k, v in cands[best].items()})
 
 
 def main():

@@ -118,8 +118,12 @@ typedef struct gat_config {
     int32_t hub_bitmaps;           /* 1: intersect against the graph's hub
                                       bitmaps where cheaper; 0: never */
     int64_t memory_budget;         /* bytes of scratch the executor may hold;
-                                      0 = 4 GiB */
-    int64_t reserved[4];
+                                      0 = 4 GiB (16 GiB for the 4-cycle
+                                      kernel's counter rows) */
+    int32_t special_kernels;       /* 1: patterns with a dedicated kernel use
+                                      it (exact 4-cycle); 0: always the plan */
+    int32_t reserved1;
+    int64_t reserved[3];
 } gat_config;
 
 /* Defaults: the reference's generated default_config.hpp
@@ -247,6 +251,29 @@ int gat_batch_run(gat_batch *b, gat_stats *stats);
 int gat_batch_counts(const gat_batch *b, uint64_t *counts, size_t n);
 int gat_batch_size(const gat_batch *b);
 void gat_batch_free(gat_batch *b);
+
+/* ------------------------------------------------------- cost model --
+ * Replaces the tuner's XGBoost regressor (tuning/tuning/role/modeling.py:
+ * 16-162) with a 3-layer FP32 perceptron (in -> 64 -> 64 -> 1, ReLU) whose
+ * forward, backward and Adam kernels are this library's own.  Features and
+ * targets are row-major float arrays on the host (n rows x in_features);
+ * the model predicts whatever target it was trained on (log seconds in
+ * graphautotune_b200.costmodel).  Parameters are one flat vector:
+ * W1[in][64], b1[64], W2[64][64], b2[64], w3[64], b3. */
+typedef struct gat_mlp gat_mlp;
+int gat_mlp_create(int in_features, uint64_t seed, gat_mlp **out);
+void gat_mlp_free(gat_mlp *net);
+int gat_mlp_num_params(const gat_mlp *net);
+int gat_mlp_get_params(const gat_mlp *net, float *out, int n);
+int gat_mlp_set_params(gat_mlp *net, const float *in, int n);
+int gat_mlp_predict(const gat_mlp *net, const float *X, int n, float *y);
+/* Full-batch mean squared error and its gradient (no update). */
+int gat_mlp_gradient(const gat_mlp *net, const float *X, const float *T, int n,
+                     float *grad_out, float *loss);
+/* Mini-batch Adam (beta1 0.9, beta2 0.999) over seeded shuffles. */
+int gat_mlp_train(gat_mlp *net, const float *X, const float *T, int n, int epochs,
+                  int batch, float lr, uint64_t seed, float *final_loss);
+const char *gat_mlp_last_error(void);
 
 /* ------------------------------------------------------ allocation-free --
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -1,0 +1,97 @@
+"""The learned cost model's CUDA kernels and what the trained network gains.
+
+  * gradients of gat_mlp_gradient equal the float64 numpy restatement
+    (oracle/mlp_ref.py) for random parameters and data
+  * Adam training on the GPU fits a known smooth function
+  * trained on engine timings from some graphs, the network's pick of a launch
+    configuration on held-out graphs runs faster than a configuration chosen
+    without it (the mean over the candidate set, i.e. a random pick), and its
+    predicted order correlates with the measured one
+"""
+import math
+import random
+
+import numpy as np
+import pytest
+
+import mlp_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mlp_gradients_match_cpu_reference(gat):
+    from graphautotune_b200 import costmodel
+
+    rng = np.random.default_rng(3)
+    for n_in, n in ((37, 200), (5, 33), (64, 1000)):
+        m = costmodel.MLP(n_in, seed=n)
+        X = rng.normal(size=(n, n_in)).astype(np.float32)
+        T = rng.normal(size=n).astype(np.float32)
+        g_gpu, loss_gpu = m.gradient(X, T)
+        loss_ref, g_ref = mlp_ref.loss_and_grad(m.params(), X, T, n_in)
+        assert abs(loss_gpu - loss_ref) <= 1e-4 * max(1.0, abs(loss_ref))
+        scale = np.abs(g_ref).max()
+        assert np.allclose(g_gpu, g_ref, rtol=1e-3, atol=1e-5 * scale), \
+            float(np.abs(g_gpu - g_ref).max())
+        y = m.predict(X)
+        assert np.allclose(y, mlp_ref.forward(m.params(), X, n_in)[0], rtol=1e-4, atol=1e-4)
+
+
+def test_mlp_training_fits_a_smooth_function(gat):
+    from graphautotune_b200 import costmodel
+
+    rng = np.random.default_rng(0)
+    X = rng.uniform(-1, 1, size=(4000, 8)).astype(np.float32)
+    T = (np.sin(2 * X[:, 0]) + X[:, 1] * X[:, 2] + 0.5 * np.abs(X[:, 3])).astype(np.float32)
+    m = costmodel.MLP(8, seed=1)
+    before = float(np.mean((m.predict(X) - T) ** 2))
+    after = m.train(X, T, epochs=150, batch=128, lr=3e-3, seed=2)
+    assert after < 0.1 * before and after < 0.02, (before, after)
+
+
+def test_trained_model_beats_choosing_without_it(gat):
+    from graphautotune_b200 import costmodel, tuner
+    from graphautotune_b200.experiments import make_graph
+
+    specs = costmodel.training_graphs(10, seed0=5000)
+    graphs = []
+    for sp in specs:
+        gr = make_graph(sp)
+        gr.upload(degree_order=True)
+        graphs.append((gr, costmodel.graph_features(gr)))
+    pats = ["0111101111011110", "0101101001011010", "0100110110010110110010100",
+            "0111110111110111110111110"]
+    scheds = [gat.Schedule(p, "exact") for p in pats]
+    pfs = [costmodel.plan_features(s) for s in scheds]
+    rng = random.Random(0)
+    cands = [tuner.default_point()]
+    while len(cands) < 16:
+        d = tuner.random_point(rng)
+        if all(tuner.fingerprint(d) != tuner.fingerprint(c) for c in cands):
+            cands.append(d)
+    execs = [gat.Executor(tuner.to_config(d)) for d in cands]
+    groups = []  # (graph index, X rows, measured ms)
+    for gi, (gr, gf) in enumerate(graphs):
+        for si, s in enumerate(scheds):
+            times = []
+            for ex in execs:
+                ex.count(gr, s)
+                times.append(min(ex.count(gr, s).kernel_ms for _ in range(2)))
+            X = np.stack([costmodel.features(gf, pfs[si], d) for d in cands])
+            groups.append((gi, X, np.array(times)))
+    train = [x for x in groups if x[0] < 7]
+    test = [x for x in groups if x[0] >= 7]
+    Xtr = np.concatenate([x[1] for x in train])
+    Ttr = np.log(np.concatenate([x[2] for x in train])).astype(np.float32)
+    model, _ = costmodel.CostModel.fit(Xtr, Ttr, epochs=300, seed=0, lr=2e-3)
+    gains, corrs = [], []
+    for _, X, times in test:
+        pred = model.predict(X)
+        pick = int(np.argmin(pred))
+        gains.append(float(np.mean(times)) / times[pick])
+        corrs.append(float(np.corrcoef(np.argsort(np.argsort(pred)),
+                                       np.argsort(np.argsort(times)))[0, 1]))
+    # geometric-mean gain of the model's pick over a pick made without it
+    gm = math.exp(sum(math.log(x) for x in gains) / len(gains))
+    assert gm > 1.1, (gains, corrs)
+    assert float(np.mean(corrs)) > 0.3, corrs

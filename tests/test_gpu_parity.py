@@ -157,6 +157,32 @@ def test_hub_bitmap_path(gat, oracle, golden_schedules, executors):
                 assert ex.count(g, gat.Schedule(p, "ref")).count == ref_want, (kind, p)
 
 
+def test_four_cycle_wedge_kernel_equals_plan(gat, oracle, golden_graphs):
+    """The exact 4-cycle count has a dedicated wedge-aggregation kernel; it
+    must equal the oracle and the generic plan (special_kernels=0), for
+    whole graphs, root ranges and shards, and on repeated calls (its counter
+    rows must come back zeroed)."""
+    c4 = "0101101001011010"
+    s = gat.Schedule(c4, "exact")
+    wedge = [_executor(gat, threads_per_warp=t, threads_per_block=b, chunk=c)
+             for t, b, c in ((32, 256, 8), (8, 128, 1), (4, 64, 32))]
+    plan = _executor(gat, special_kernels=0)
+    graphs = list(golden_graphs.values()) + [gat.Graph.rmat(12, 1 << 15, 0.57, 0.19, 0.19, 5),
+                                             gat.Graph.barabasi_albert(4000, 6, 8)]
+    for g in graphs:
+        off, adj = g.csr()
+        want = oracle.exact_count(off, adj, c4) if len(off) < 5000 else plan.count(g, s).count
+        assert plan.count(g, s).count == want
+        for ex in wedge:
+            for _ in range(2):
+                assert ex.count(g, s).count == want
+        V = len(off) - 1
+        bounds = [0, V // 5, V // 2, V]
+        assert sum(wedge[0].count_range(g, s, a, b)[0] for a, b in zip(bounds, bounds[1:])) \
+            == want
+        assert sum(wedge[1].count_shard(g, s, r, 3)[0] for r in range(3)) == want
+
+
 def test_relabelling_and_sharding_invariance(gat, executors):
     """Size-independent properties: the exact count does not depend on the
     vertex ids (degree-ordered vs given ids), and root-range shards sum to

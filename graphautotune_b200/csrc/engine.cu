@@ -285,11 +285,24 @@ __device__ __forceinline__ int ceil_log2(int x) {
     return x <= 1 ? 1 : 32 - __clz(x - 1);
 }
 
-// Builds every prefix set that ends at level k for candidate v.
+// |{u in N(v) : u < T}|.  Cut at v itself it is v's lower degree, one read
+// of the lower-neighbour offsets (rows are sorted); otherwise a search.
+template <int G>
+__device__ __forceinline__ int32_t cut_neighbours(const Tile<G> &t, const SearchArgs &a,
+                                                  int32_t v, const int32_t *nb, int32_t dv,
+                                                  int32_t T) {
+    if (T == kInf) return dv;
+    if (T == v && a.lo_off != nullptr) return (int32_t)(a.lo_off[v + 1] - a.lo_off[v]);
+    return tile_bound<G, false>(t, nb, dv, T);
+}
+
+// Builds every prefix set that ends at level k for candidate v.  `cand_idx`
+// is v's position in the list it was drawn from (the loop set of level k),
+// or -1: that list cut at v is exactly its first cand_idx elements.
 template <int G, bool STATS>
 __device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
                            const SearchArgs &a, int k, int32_t v, bool collided,
-                           int32_t *scratch, unsigned long long &bytes) {
+                           int32_t *scratch, unsigned long long &bytes, int cand_idx = -1) {
     const int64_t o = a.off[v];
     const int32_t *nb = a.adj + o;
     const int32_t dv = (int32_t)(a.off[v + 1] - o);
@@ -305,15 +318,20 @@ __device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
             if (kind == GAT_SET_ALIAS) {
                 ptr = nb;
                 owner = v;
-                len = (T == kInf) ? dv : tile_bound<G, false>(t, nb, dv, T);
+                len = cut_neighbours(t, a, v, nb, dv, T);
             } else {
                 const int f = P.p_father[p];
                 const int32_t *fp = S.sp[f];
                 int32_t fl = S.sl[f];
                 // F is already cut at its own bound; cut again only when this
-                // set's bound is a different expression.
-                if (T != kInf && P.p_trunc[p] != P.p_trunc[f])
-                    fl = tile_bound<G, false>(t, fp, fl, T);
+                // set's bound is a different expression.  When F is the list
+                // v was drawn from and the bound is v, the cut is v's index.
+                if (T != kInf) {
+                    if (cand_idx >= 0 && T == v && f == P.l_loop[k])
+                        fl = min(fl, cand_idx);
+                    else if (P.p_trunc[p] != P.p_trunc[f])
+                        fl = tile_bound<G, false>(t, fp, fl, T);
+                }
                 // Cheapest way to intersect: probe F into v's bitmap, probe
                 // N(v) into the bitmap of F's owner, or binary-search the
                 // shorter list in the longer one.  Probe lists are cut at T,
@@ -331,9 +349,9 @@ __device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
                     row = a.bitmaps + (int64_t)hub_v * a.bitmap_words;
                     probe = fp;
                     np = fl;
-                    if (STATS && T != kInf) nl = tile_bound<G, false>(t, nb, dv, T);
+                    if (STATS) nl = cut_neighbours(t, a, v, nb, dv, T);
                 } else {
-                    if (T != kInf) nl = tile_bound<G, false>(t, nb, dv, T);
+                    nl = cut_neighbours(t, a, v, nb, dv, T);
                     const int shorter = min(nl, fl), longer = max(nl, fl);
                     const long long bs_cost = (long long)shorter * ceil_log2(longer + 1);
                     if (hub_v >= 0 && (long long)fl <= bs_cost &&
@@ -453,7 +471,8 @@ __device__ __forceinline__ void run_units(const Tile<G> &t, TileSmem &S, const G
         }
         if (t.lane == 0) S.v[1] = v1;
         t.sync();
-        level_sets<G, STATS>(t, S, P, a, 1, v1, false, scratch, bytes);
+        level_sets<G, STATS>(t, S, P, a, 1, v1, false, scratch, bytes,
+                             (int)(tk - task_off[v0]));
         if (basic == 2) {
             const long long r = iep_value(t, S, P, a.linear_below);
             if (t.lane == 0) acc += (unsigned long long)r;
@@ -483,7 +502,7 @@ __device__ __forceinline__ void run_units(const Tile<G> &t, TileSmem &S, const G
             }
             if (t.lane == 0) S.v[k] = cand;
             t.sync();
-            level_sets<G, STATS>(t, S, P, a, k, cand, hit, scratch, bytes);
+            level_sets<G, STATS>(t, S, P, a, k, cand, hit, scratch, bytes, S.pos[k] - 1);
             if (k == basic - 1) {
                 const long long r = iep_value(t, S, P, a.linear_below);
                 if (t.lane == 0) acc += (unsigned long long)r;

@@ -316,13 +316,13 @@ class Executor(_Handle):
                                       st.tile, st.scratch_bytes)
 
     def count_shard(self, graph: Graph, schedule: Schedule, shard: int, num_shards: int,
-                    stream: int | None = None) -> tuple[int, CountResult]:
+                    stream: int | None = None, balg: bool = False) -> tuple[int, CountResult]:
         """Undivided signed total of one equal slice of the work queue."""
         raw = C.c_int64()
         st = gat_stats()
-        check(lib().gat_executor_count_shard(self._h, graph._h, schedule._h,
-                                             C.c_void_p(stream) if stream else None,
-                                             shard, num_shards, C.byref(raw), C.byref(st)))
+        fn = lib().gat_executor_count_shard_balg if balg else lib().gat_executor_count_shard
+        check(fn(self._h, graph._h, schedule._h, C.c_void_p(stream) if stream else None,
+                 shard, num_shards, C.byref(raw), C.byref(st)))
         return raw.value, CountResult(raw.value, st.kernel_ms, st.total_ms, st.raw_sum,
                                       st.divisor, st.tasks, st.balg_bytes, st.grid, st.block,
                                       st.tile, st.scratch_bytes)

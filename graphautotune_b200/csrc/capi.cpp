@@ -797,6 +797,7 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
         e->scratch_bytes = need;
     }
     *e->h_plan = plan;
+    if (e->cfg.special_kernels == 0) e->h_plan->lane_last = 0;
     if ((ce = cudaMemcpyAsync(e->d_plan, e->h_plan, sizeof(GatPlan), cudaMemcpyHostToDevice,
                               strm)) != cudaSuccess)
         return cuda_fail(ce, "plan upload");
@@ -864,6 +865,16 @@ int gat_executor_count_shard(gat_executor *e, gat_graph *g, const gat_schedule *
     if (num_shards < 1) return fail(GAT_ERR_ARGUMENT, "num_shards must be >= 1");
     uint64_t c = 0;
     int rc = count_impl(e, g, s, stream, &c, stats, false, -1, -1, shard, num_shards);
+    if (rc == GAT_OK && raw_sum) *raw_sum = (int64_t)c;
+    return rc;
+}
+
+int gat_executor_count_shard_balg(gat_executor *e, gat_graph *g, const gat_schedule *s,
+                                  void *stream, int32_t shard, int32_t num_shards,
+                                  int64_t *raw_sum, gat_stats *stats) {
+    if (num_shards < 1) return fail(GAT_ERR_ARGUMENT, "num_shards must be >= 1");
+    uint64_t c = 0;
+    int rc = count_impl(e, g, s, stream, &c, stats, true, -1, -1, shard, num_shards);
     if (rc == GAT_OK && raw_sum) *raw_sum = (int64_t)c;
     return rc;
 }
@@ -996,6 +1007,7 @@ int gat_batch_prepare(gat_batch *b, const gat_config *c, int use_cuda_graph) {
         v.bitmaps = dc.bitmaps;
         v.bitmap_words = dc.bitmap_words;
         plans[j] = s->plan.plan;
+        if (b->cfg.special_kernels == 0) plans[j].lane_last = 0;
         batch_fill_job(host_jobs.data() + j * jb, b->d_plans + j, plans[j], v,
                        b->cfg.set_search_type, b->cfg.hub_bitmaps != 0);
         stride = std::max<int64_t>(stride, tile_scratch_ints(plans[j], v.max_degree));

@@ -443,6 +443,165 @@ __device__ long long iep_value(const Tile<G> &t, TileSmem &S, const GatPlan &P,
     return (long long)local;
 }
 
+// One lane alone: first i in a[0, n) with a[i] >= x.
+__device__ __forceinline__ int lower_serial(const int32_t *a, int n, int32_t x) {
+    int lo = 0;
+    while (n > 0) {
+        const int h = n >> 1;
+        const bool right = a[lo + h] < x;
+        lo = right ? lo + h + 1 : lo;
+        n = right ? n - h - 1 : h;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int32_t cut_serial(const SearchArgs &a, int32_t v,
+                                              const int32_t *nb, int32_t dv, int32_t T) {
+    if (T == kInf) return dv;
+    if (T == v && a.lo_off != nullptr) return (int32_t)(a.lo_off[v + 1] - a.lo_off[v]);
+    return lower_serial(nb, dv, T);
+}
+
+// y equals one of the levels in `ex` (bit k stands for the lane's candidate).
+__device__ __forceinline__ bool excluded(const TileSmem &S, unsigned ex, int k, int32_t cand,
+                                         int32_t y) {
+    bool r = ((ex >> k) & 1u) && y == cand;
+    unsigned m = ex & ~(1u << k);
+    while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1;
+        r |= (S.v[j] == y);
+    }
+    return r;
+}
+
+// Last level with one candidate per lane (plans with lane_last set).  Every
+// set of level k = basic-1 is a count |N(cand) n F| whose father F belongs
+// to an earlier level, and the unit's IEP value needs only those counts, so
+// lane i takes candidates i, i+G, ... of the level's loop list and forms its
+// counts and IEP value alone: no shared-memory state, no syncs and no idle
+// lanes when the lists are shorter than the tile.  Each count is the same
+// intersection, with the same bounds, exclusions and bitmap choice, that
+// level_sets would form for that candidate.  Returns the sum of the
+// candidates' IEP values on every lane.
+template <int G, bool STATS>
+__device__ unsigned long long lane_last_level(const Tile<G> &t, const TileSmem &S,
+                                              const GatPlan &P, const SearchArgs &a, int k,
+                                              unsigned long long &bytes) {
+    const int32_t *src = S.src[k];
+    const int32_t cnt = S.cnt[k];
+    const unsigned kbit = 1u << k;
+    const int loop = P.l_loop[k];
+    unsigned long long sum = 0, by = 0;
+    long long val[8];
+    for (int i = t.lane; i < cnt; i += G) {
+        const int32_t cand = src[i];
+        bool hit = false;
+        unsigned dm = P.l_distinct[k];
+        while (dm) {
+            const int j = __ffs(dm) - 1;
+            dm &= dm - 1;
+            hit |= (S.v[j] == cand);
+        }
+        // Skipped (exact) or all its sets cleared (reference mode): adds 0.
+        if (hit) continue;
+        const int64_t o = a.off[cand];
+        const int32_t *nb = a.adj + o;
+        const int32_t dv = (int32_t)(a.off[cand + 1] - o);
+        const int hub_v = (a.hub_slot != nullptr) ? a.hub_slot[cand] : -1;
+        for (int x = 0; x < P.iep_num; x++) {
+            const int p = P.iep_prefix[x];
+            const unsigned tm = P.p_trunc[p];
+            int32_t T = min_of(S, tm & ~kbit);
+            if (tm & kbit) T = min(T, cand);
+            const int f = P.p_father[p];
+            const int32_t *fp = S.sp[f];
+            int32_t fl = S.sl[f];
+            if (T != kInf) {
+                if (T == cand && f == loop)
+                    fl = min(fl, i);
+                else if (tm != P.p_trunc[f])
+                    fl = lower_serial(fp, fl, T);
+            }
+            const int owner_f = S.owner[f];
+            const int hub_f =
+                (a.hub_slot != nullptr && owner_f >= 0) ? a.hub_slot[owner_f] : -1;
+            const uint32_t *row = nullptr;
+            const int32_t *probe = nullptr;
+            int np = 0;
+            int32_t nl = dv;
+            if (hub_v >= 0 && fl <= dv) {
+                row = a.bitmaps + (int64_t)hub_v * a.bitmap_words;
+                probe = fp;
+                np = fl;
+                if (STATS) nl = cut_serial(a, cand, nb, dv, T);
+            } else {
+                nl = cut_serial(a, cand, nb, dv, T);
+                const int shorter = min(nl, fl), longer = max(nl, fl);
+                const long long bs_cost = (long long)shorter * ceil_log2(longer + 1);
+                if (hub_v >= 0 && (long long)fl <= bs_cost && (hub_f < 0 || fl <= nl)) {
+                    row = a.bitmaps + (int64_t)hub_v * a.bitmap_words;
+                    probe = fp;
+                    np = fl;
+                } else if (hub_f >= 0 && (long long)nl <= bs_cost) {
+                    row = a.bitmaps + (int64_t)hub_f * a.bitmap_words;
+                    probe = nb;
+                    np = nl;
+                }
+            }
+            if (STATS) by += 4ull * (unsigned)(nl + fl);
+            const unsigned ex = P.p_excl[p];
+            int c = 0;
+            if (row) {
+                for (int e = 0; e < np; e++) {
+                    const int32_t y = probe[e];
+                    c += (bit_set(row, y) && !excluded(S, ex, k, cand, y)) ? 1 : 0;
+                }
+            } else {
+                const int32_t *sa = nl <= fl ? nb : fp;
+                const int32_t *lb = nl <= fl ? fp : nb;
+                const int ns = min(nl, fl), nlong = max(nl, fl);
+                for (int e = 0; e < ns; e++) {
+                    const int32_t y = sa[e];
+                    c += (contains(lb, nlong, y, a.linear_below) &&
+                          !excluded(S, ex, k, cand, y))
+                             ? 1
+                             : 0;
+                }
+            }
+            val[x] = c;
+        }
+        unsigned long long local = 0, cur = 1;
+        int last = -1;
+        for (int g = 0; g < P.num_terms; g++) {
+            const unsigned long long v = (unsigned long long)val[P.t_slot[g]];
+            cur = (g == last + 1) ? v : cur * v;
+            if (P.t_close[g]) {
+                last = g;
+                local += cur * (unsigned long long)(long long)P.t_coef[g];
+            }
+        }
+        sum += local;
+    }
+    if (STATS) {
+        by = t.sum(by);
+        if (t.lane == 0) bytes += by;
+    }
+    return t.sum(sum);
+}
+
+// The lane path pays when the candidates fill at least half the tile, or
+// outnumber the elements of the longest father list (the cooperative path
+// would then leave most lanes idle on every candidate).
+template <int G>
+__device__ __forceinline__ bool lane_worth(const TileSmem &S, const GatPlan &P, int k) {
+    const int32_t cnt = S.cnt[k];
+    if (2 * cnt >= G) return true;
+    int32_t fmax = 0;
+    for (int x = 0; x < P.iep_num; x++) fmax = max(fmax, S.sl[P.p_father[P.iep_prefix[x]]]);
+    return cnt >= fmax;
+}
+
 // Runs the level-1 units [start, end) of one job: each unit (v0, v1) is the
 // start of a depth-first walk over levels 2 .. basic-1.  Lane 0 of the tile
 // accumulates the units' IEP values in `acc`.
@@ -480,6 +639,11 @@ __device__ __forceinline__ void run_units(const Tile<G> &t, TileSmem &S, const G
             continue;
         }
         setup_level(t, S, P, 2);
+        if (basic == 3 && P.lane_last && lane_worth<G>(S, P, 2)) {
+            const unsigned long long r = lane_last_level<G, STATS>(t, S, P, a, 2, bytes);
+            if (t.lane == 0) acc += r;
+            continue;
+        }
         int k = 2;
         while (k >= 2) {
             if (S.pos[k] >= S.cnt[k]) {
@@ -510,6 +674,12 @@ __device__ __forceinline__ void run_units(const Tile<G> &t, TileSmem &S, const G
                 continue;
             }
             setup_level(t, S, P, k + 1);
+            if (k + 1 == basic - 1 && P.lane_last && lane_worth<G>(S, P, k + 1)) {
+                const unsigned long long r =
+                    lane_last_level<G, STATS>(t, S, P, a, k + 1, bytes);
+                if (t.lane == 0) acc += r;
+                continue;
+            }
             k++;
         }
     }

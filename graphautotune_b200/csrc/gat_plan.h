@@ -46,6 +46,10 @@ typedef struct GatPlan {
                               exact 4-cycle count has a dedicated kernel
                               (the plan stays valid as its fallback) */
     int64_t divisor;       /* final count = sum / divisor */
+    int32_t lane_last;     /* 1: every prefix of level basic-1 is COUNT and
+                              every IEP slot is one of them (<= 8 slots), so
+                              lanes may take last-level candidates one each */
+    int32_t pad1;
 
     int8_t p_level[GAT_MAX_PREFIX];
     int8_t p_father[GAT_MAX_PREFIX];

@@ -232,6 +232,12 @@ int gat_executor_count_shard(gat_executor *e, gat_graph *g,
                              const gat_schedule *s, void *stream,
                              int32_t shard, int32_t num_shards,
                              int64_t *raw_sum, gat_stats *stats);
+/* As gat_executor_count_shard, with the algorithmic bytes of the slice's
+ * set operations measured as in gat_executor_count_balg. */
+int gat_executor_count_shard_balg(gat_executor *e, gat_graph *g,
+                                  const gat_schedule *s, void *stream,
+                                  int32_t shard, int32_t num_shards,
+                                  int64_t *raw_sum, gat_stats *stats);
 /* ---------------------------------------------------------------- batch --
  * No single reference counterpart: the reference runs one pm process per
  * (pattern, graph, config) (tuning/tuning/role/driver.py:88-132).  A batch

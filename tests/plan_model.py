@@ -21,6 +21,7 @@ class GatPlan(C.Structure):
         ("mode", C.c_int32), ("collide_clear", C.c_int32), ("level1_bounded", C.c_int32),
         ("num_store", C.c_int32), ("iep_num", C.c_int32), ("num_terms", C.c_int32),
         ("special", C.c_int32), ("divisor", C.c_int64),
+        ("lane_last", C.c_int32), ("pad1", C.c_int32),
         ("p_level", C.c_int8 * MAXP), ("p_father", C.c_int8 * MAXP),
         ("p_kind", C.c_int8 * MAXP), ("p_slot", C.c_int8 * MAXP),
         ("p_trunc", C.c_uint16 * MAXP), ("p_excl", C.c_uint16 * MAXP),

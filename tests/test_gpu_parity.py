@@ -201,3 +201,39 @@ def test_relabelling_and_sharding_invariance(gat, executors):
         raw = sum(executors[0].count_range(g1, s, lo, hi)[0]
                   for lo, hi in zip(bounds, bounds[1:]))
         assert raw == a.raw_sum and raw // a.divisor == a.count, p
+
+
+def test_lane_last_level_equals_tile_path(gat, oracle, golden_schedules):
+    """The one-candidate-per-lane last level (special_kernels=1) gives the
+    same counts and the same algorithmic byte totals as the tile-cooperative
+    path (special_kernels=0), on every tile width, with and without hub
+    bitmaps, in both modes."""
+    shapes = ((32, 256, 8), (8, 128, 1), (1, 128, 16))
+    lanes = [_executor(gat, threads_per_warp=t, threads_per_block=b, chunk=c)
+             for t, b, c in shapes]
+    tiles = [_executor(gat, threads_per_warp=t, threads_per_block=b, chunk=c,
+                       special_kernels=0) for t, b, c in shapes]
+    pats = [p for p in NAMED + gat.enumerate_patterns(5)
+            if p != "0101101001011010"]  # the 4-cycle has its own kernel
+    graphs = [_graph(gat, *m) for m in MEDIUM]
+    hubby = gat.Graph.rmat(12, 1 << 15, 0.57, 0.19, 0.19, 9)
+    hubby.upload(degree_order=True, hub_min_degree=8, hub_max_bytes=1 << 28)
+    graphs.append(hubby)
+    for g in graphs:
+        off, adj = g.csr()
+        for p in pats:
+            for mode in ("exact", "ref"):
+                s = gat.Schedule(p, mode)
+                if mode == "ref":
+                    sd = golden_schedules.get(p)
+                    if sd is None or sd.get("crash") or oracle.ref_engine(off, adj, sd)[0] != 0:
+                        continue
+                want = None
+                for a, b in zip(lanes, tiles):
+                    ra, rb = a.count(g, s, balg=True), b.count(g, s, balg=True)
+                    assert ra.count == rb.count, (p, mode)
+                    assert ra.balg_bytes == rb.balg_bytes, (p, mode)
+                    want = ra.count if want is None else want
+                    assert ra.count == want, (p, mode)
+                if mode == "exact" and len(off) <= 2001:
+                    assert want == oracle.exact_count(off, adj, p), p

@@ -450,21 +450,25 @@ def run_ours(args):
 
 def run_profile_case(args):
     """A bounded slice of one workload pattern's search, for profilers: the
-    workload graph, `pattern` counted over shard 0 of `parts` equal slices of
-    the work queue, warmup + steps launches (one search kernel each)."""
+    workload graph, `pattern` counted over one shard (default 0) of `parts`
+    equal slices of the work queue (`--profile PATTERN:PARTS[:SHARD]`),
+    warmup + steps launches (one search kernel each)."""
     import torch
 
     import graphautotune_b200 as g
 
-    name, parts = args.profile.split(":")
+    fields = args.profile.split(":")
+    name, parts = fields[0], int(fields[1])
+    shard = int(fields[2]) if len(fields) > 2 else 0
     torch.cuda.set_device(0)
     gr, _ = load_workload_graph(g)
     gr.upload(degree_order=True)
     ex = g.Executor(g.Config.engine_default())
     s = g.Schedule(PATTERNS[name], "exact", stats_graph=gr)
     for i in range(args.warmup + args.steps):
-        raw, r = ex.count_shard(gr, s, 0, int(parts))
-        log(f"{name} shard 0/{parts}: raw {raw} tasks {r.tasks} kernel {r.kernel_ms:.2f} ms")
+        raw, r = ex.count_shard(gr, s, shard, parts)
+        log(f"{name} shard {shard}/{parts}: raw {raw} tasks {r.tasks} "
+            f"kernel {r.kernel_ms:.2f} ms")
     return 0
 
 
@@ -475,7 +479,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--profile", default=None,
-                    help="PATTERN:PARTS, e.g. c4:16 - one slice of the search, for ncu")
+                    help="PATTERN:PARTS[:SHARD], e.g. c4:64:32 - one slice of the search, for ncu")
     args = ap.parse_args()
     if args.profile:
         sys.exit(run_profile_case(args))

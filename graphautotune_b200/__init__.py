@@ -264,6 +264,15 @@ class Graph(_Handle):
         check(lib().gat_graph_hubs(self._h, 1 if ordered else 0, C.byref(n)))
         return n.value
 
+    def ordered_csr(self) -> tuple[np.ndarray, np.ndarray]:
+        """The degree-ordered device copy (vertex r = r-th by decreasing
+        degree, ties by id), read back from the GPU."""
+        V, E, _ = self.info()
+        off = np.empty(V + 1, np.int64)
+        adj = np.empty(max(E, 1), np.int32)
+        check(lib().gat_graph_ordered_csr(self._h, off.ctypes.data, adj.ctypes.data))
+        return off, adj[:E]
+
 
 @dataclass
 class CountResult:

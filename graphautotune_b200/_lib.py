@@ -103,6 +103,7 @@ _SIGS = {
     "gat_graph_upload": (C.c_int, [P, C.c_int, P]),
     "gat_graph_upload_ex": (C.c_int, [P, C.c_int, C.c_int64, C.c_int64, P]),
     "gat_graph_hubs": (C.c_int, [P, C.c_int, C.POINTER(C.c_int32)]),
+    "gat_graph_ordered_csr": (C.c_int, [P, P, P]),
     "gat_graph_free": (None, [P]),
     "gat_executor_create": (C.c_int, [C.POINTER(gat_config), C.POINTER(P)]),
     "gat_executor_free": (None, [P]),

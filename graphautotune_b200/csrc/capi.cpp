@@ -477,61 +477,106 @@ int gat_graph_csr(const gat_graph *g, const int64_t **offsets, const int32_t **a
 }
 
 namespace {
+// Completes a device copy whose off and adj are in place: lo_off is derived
+// on the device, and both offset arrays are kept on the host too (range and
+// shard arithmetic reads them).  `off_known` is the host's copy of off when
+// there is one; otherwise off is read back.
+int finish_copy(DevCopy &d, int32_t V, int32_t max_degree, const std::vector<int64_t> *off_known,
+                cudaStream_t st) {
+    cudaError_t e;
+    if ((e = cudaMalloc(&d.lo_off, sizeof(int64_t) * (size_t(V) + 1))) != cudaSuccess) {
+        d.release();
+        return fail(GAT_ERR_MEMORY, std::string("device graph allocation: ") + cudaGetErrorString(e));
+    }
+    d.lo_host.resize(size_t(V) + 1);
+    if (off_known)
+        d.off_host = *off_known;
+    else
+        d.off_host.resize(size_t(V) + 1);
+    if ((e = lower_offsets_device(d.off, d.adj, V, d.lo_off, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d.lo_host.data(), d.lo_off, sizeof(int64_t) * (size_t(V) + 1),
+                             cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (!off_known &&
+         (e = cudaMemcpyAsync(d.off_host.data(), d.off, sizeof(int64_t) * (size_t(V) + 1),
+                              cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        d.release();
+        return cuda_fail(e, "graph upload");
+    }
+    d.lo_total = d.lo_host[size_t(V)];
+    d.max_degree = max_degree;
+    d.ready = true;
+    return GAT_OK;
+}
+
 int upload_copy(const HostGraph &h, DevCopy &d, cudaStream_t st) {
     d.release();
-    std::vector<int64_t> lo(size_t(h.V) + 1, 0);
-    for (int32_t v = 0; v < h.V; v++) {
-        auto b = h.adj.begin() + h.off[v], e = h.adj.begin() + h.off[v + 1];
-        lo[v + 1] = lo[v] + (std::lower_bound(b, e, v) - b);
-    }
     cudaError_t e;
     if ((e = cudaMalloc(&d.off, sizeof(int64_t) * (h.V + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&d.adj, sizeof(int32_t) * std::max<int64_t>(h.E, 1))) != cudaSuccess ||
-        (e = cudaMalloc(&d.lo_off, sizeof(int64_t) * (h.V + 1))) != cudaSuccess) {
+        (e = cudaMalloc(&d.adj, sizeof(int32_t) * std::max<int64_t>(h.E, 1))) != cudaSuccess) {
         d.release();
         return fail(GAT_ERR_MEMORY, std::string("device graph allocation: ") + cudaGetErrorString(e));
     }
     if ((e = cudaMemcpyAsync(d.off, h.off.data(), sizeof(int64_t) * (h.V + 1),
                              cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (h.E > 0 && (e = cudaMemcpyAsync(d.adj, h.adj.data(), sizeof(int32_t) * h.E,
-                                         cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
-        (e = cudaMemcpyAsync(d.lo_off, lo.data(), sizeof(int64_t) * (h.V + 1),
-                             cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+                                         cudaMemcpyHostToDevice, st)) != cudaSuccess)) {
         d.release();
         return cuda_fail(e, "graph upload");
     }
-    d.lo_total = lo[h.V];
-    d.lo_host = std::move(lo);
-    d.off_host = h.off;
-    d.max_degree = h.max_degree();
-    d.ready = true;
-    return GAT_OK;
+    return finish_copy(d, h.V, h.max_degree(), &h.off, st);
+}
+
+// The degree-ordered copy, derived on the device from the resident copy
+// `src` of h (graphs whose edge count CUB's segmented sort cannot index are
+// relabelled on the host and uploaded instead).
+int derive_ordered_copy(const HostGraph &h, const DevCopy &src, DevCopy &d, cudaStream_t st) {
+    if (!relabel_fits_device(h.V, h.E)) {
+        HostGraph r;
+        relabel_by_degree(h, r, nullptr);
+        return upload_copy(r, d, st);
+    }
+    d.release();
+    cudaError_t e;
+    if ((e = cudaMalloc(&d.off, sizeof(int64_t) * (h.V + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&d.adj, sizeof(int32_t) * std::max<int64_t>(h.E, 1))) != cudaSuccess) {
+        d.release();
+        return fail(GAT_ERR_MEMORY, std::string("device graph allocation: ") + cudaGetErrorString(e));
+    }
+    const int32_t md = h.max_degree();
+    if ((e = relabel_by_degree_device(src.off, src.adj, h.V, h.E, md, d.off, d.adj, st)) !=
+        cudaSuccess) {
+        d.release();
+        return cuda_fail(e, "degree relabel");
+    }
+    return finish_copy(d, h.V, md, nullptr, st);
 }
 
 // Hub bitmaps for the vertices of degree >= min_degree, largest degree first,
 // as many as fit in max_bytes.
-int upload_hubs(const HostGraph &h, DevCopy &d, int64_t min_degree, int64_t max_bytes,
+int upload_hubs(DevCopy &d, int32_t V, int64_t min_degree, int64_t max_bytes,
                 cudaStream_t st) {
-    if (min_degree <= 0 || max_bytes <= 0 || h.V == 0) return GAT_OK;
-    const int64_t words = (int64_t(h.V) + 31) / 32;
+    if (min_degree <= 0 || max_bytes <= 0 || V == 0) return GAT_OK;
+    const std::vector<int64_t> &off = d.off_host;
+    auto degree = [&](int32_t v) { return off[size_t(v) + 1] - off[size_t(v)]; };
+    const int64_t words = (int64_t(V) + 31) / 32;
     std::vector<int32_t> cand;
-    for (int32_t v = 0; v < h.V; v++)
-        if (h.degree(v) >= min_degree) cand.push_back(v);
+    for (int32_t v = 0; v < V; v++)
+        if (degree(v) >= min_degree) cand.push_back(v);
     std::stable_sort(cand.begin(), cand.end(),
-                     [&](int32_t x, int32_t y) { return h.degree(x) > h.degree(y); });
+                     [&](int32_t x, int32_t y) { return degree(x) > degree(y); });
     const int64_t fit = max_bytes / (words * 4);
     if ((int64_t)cand.size() > fit) cand.resize(size_t(fit));
     if (cand.empty()) return GAT_OK;
-    std::vector<int32_t> slot(size_t(h.V), -1);
+    std::vector<int32_t> slot(size_t(V), -1);
     for (size_t i = 0; i < cand.size(); i++) slot[cand[i]] = (int32_t)i;
     cudaError_t e;
     const size_t bm_bytes = size_t(cand.size()) * size_t(words) * 4;
-    if ((e = cudaMalloc(&d.hub_slot, sizeof(int32_t) * h.V)) != cudaSuccess ||
+    if ((e = cudaMalloc(&d.hub_slot, sizeof(int32_t) * V)) != cudaSuccess ||
         (e = cudaMalloc(&d.hubs, sizeof(int32_t) * cand.size())) != cudaSuccess ||
         (e = cudaMalloc(&d.bitmaps, bm_bytes)) != cudaSuccess)
         return fail(GAT_ERR_MEMORY, std::string("hub bitmap allocation: ") + cudaGetErrorString(e));
-    if ((e = cudaMemcpyAsync(d.hub_slot, slot.data(), sizeof(int32_t) * h.V,
+    if ((e = cudaMemcpyAsync(d.hub_slot, slot.data(), sizeof(int32_t) * V,
                              cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(d.hubs, cand.data(), sizeof(int32_t) * cand.size(),
                              cudaMemcpyHostToDevice, st)) != cudaSuccess ||
@@ -553,15 +598,14 @@ int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    const int32_t V = g->host.V;
     int rc = upload_copy(g->host, g->dev, st);
-    if (rc == GAT_OK) rc = upload_hubs(g->host, g->dev, hub_min_degree, hub_max_bytes, st);
+    if (rc == GAT_OK) rc = upload_hubs(g->dev, V, hub_min_degree, hub_max_bytes, st);
     if (rc != GAT_OK) return rc;
     if (flags & GAT_UPLOAD_DEGREE_ORDER) {
-        HostGraph r;
-        relabel_by_degree(g->host, r, nullptr);
-        rc = upload_copy(r, g->dev_ordered, st);
+        rc = derive_ordered_copy(g->host, g->dev, g->dev_ordered, st);
         if (rc == GAT_OK)
-            rc = upload_hubs(r, g->dev_ordered, hub_min_degree, hub_max_bytes, st);
+            rc = upload_hubs(g->dev_ordered, V, hub_min_degree, hub_max_bytes, st);
         if (rc != GAT_OK) return rc;
     } else {
         g->dev_ordered.release();
@@ -578,6 +622,19 @@ int gat_graph_upload(gat_graph *g, int flags, void *stream) {
 int gat_graph_hubs(const gat_graph *g, int ordered_copy, int32_t *nhubs) {
     if (!g || !nhubs) return fail(GAT_ERR_ARGUMENT, "null argument");
     *nhubs = ordered_copy ? g->dev_ordered.nhubs : g->dev.nhubs;
+    return GAT_OK;
+}
+
+int gat_graph_ordered_csr(const gat_graph *g, int64_t *offsets, int32_t *adj) {
+    if (!g || !offsets || !adj) return fail(GAT_ERR_ARGUMENT, "null argument");
+    const DevCopy &d = g->dev_ordered;
+    if (!d.ready) return fail(GAT_ERR_STATE, "no degree-ordered copy uploaded");
+    cudaError_t e;
+    if ((e = cudaMemcpy(offsets, d.off, sizeof(int64_t) * (size_t(g->host.V) + 1),
+                        cudaMemcpyDeviceToHost)) != cudaSuccess ||
+        (g->host.E > 0 && (e = cudaMemcpy(adj, d.adj, sizeof(int32_t) * size_t(g->host.E),
+                                          cudaMemcpyDeviceToHost)) != cudaSuccess))
+        return cuda_fail(e, "ordered copy read-back");
     return GAT_OK;
 }
 

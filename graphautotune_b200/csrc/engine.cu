@@ -476,14 +476,15 @@ __device__ __forceinline__ bool excluded(const TileSmem &S, unsigned ex, int k, 
 }
 
 // Last level with one candidate per lane (plans with lane_last set).  Every
-// set of level k = basic-1 is a count |N(cand) n F| whose father F belongs
-// to an earlier level, and the unit's IEP value needs only those counts, so
-// lane i takes candidates i, i+G, ... of the level's loop list and forms its
-// counts and IEP value alone: no shared-memory state, no syncs and no idle
-// lanes when the lists are shorter than the tile.  Each count is the same
-// intersection, with the same bounds, exclusions and bitmap choice, that
-// level_sets would form for that candidate.  Returns the sum of the
-// candidates' IEP values on every lane.
+// set of level k = basic-1 is either a count |N(cand) n F| whose father F
+// belongs to an earlier level or N(cand) itself, so nothing of level k has to
+// be stored: lane i takes candidates i, i+G, ... of the level's loop list and
+// forms that level's sets and the unit's IEP value alone (IEP slots of
+// earlier levels are read from the tile's state).  No shared-memory writes,
+// no syncs, and no idle lanes when the lists are shorter than the tile.  Each
+// set and each IEP value is formed exactly as level_sets and iep_value form
+// it for that candidate (same bounds, exclusions and bitmap-or-search
+// choice).  Returns the sum of the candidates' IEP values on every lane.
 template <int G, bool STATS>
 __device__ unsigned long long lane_last_level(const Tile<G> &t, const TileSmem &S,
                                               const GatPlan &P, const SearchArgs &a, int k,
@@ -492,8 +493,10 @@ __device__ unsigned long long lane_last_level(const Tile<G> &t, const TileSmem &
     const int32_t cnt = S.cnt[k];
     const unsigned kbit = 1u << k;
     const int loop = P.l_loop[k];
+    const int pb = P.l_pbegin[k], pe = P.l_pbegin[k + 1];
     unsigned long long sum = 0, by = 0;
-    long long val[8];
+    long long lv[8];   // level-k sets: count, or cut length of N(cand)
+    long long val[8];  // IEP slots
     for (int i = t.lane; i < cnt; i += G) {
         const int32_t cand = src[i];
         bool hit = false;
@@ -503,17 +506,25 @@ __device__ unsigned long long lane_last_level(const Tile<G> &t, const TileSmem &
             dm &= dm - 1;
             hit |= (S.v[j] == cand);
         }
-        // Skipped (exact) or all its sets cleared (reference mode): adds 0.
-        if (hit) continue;
+        // Exact plans skip a colliding candidate; reference plans keep it
+        // with every level-k set empty.
+        if (hit && !P.collide_clear) continue;
         const int64_t o = a.off[cand];
         const int32_t *nb = a.adj + o;
         const int32_t dv = (int32_t)(a.off[cand + 1] - o);
         const int hub_v = (a.hub_slot != nullptr) ? a.hub_slot[cand] : -1;
-        for (int x = 0; x < P.iep_num; x++) {
-            const int p = P.iep_prefix[x];
+        for (int p = pb; p < pe; p++) {
+            if (hit) {
+                lv[p - pb] = 0;
+                continue;
+            }
             const unsigned tm = P.p_trunc[p];
             int32_t T = min_of(S, tm & ~kbit);
             if (tm & kbit) T = min(T, cand);
+            if (P.p_kind[p] == GAT_SET_ALIAS) {
+                lv[p - pb] = cut_serial(a, cand, nb, dv, T);
+                continue;
+            }
             const int f = P.p_father[p];
             const int32_t *fp = S.sp[f];
             int32_t fl = S.sl[f];
@@ -569,7 +580,27 @@ __device__ unsigned long long lane_last_level(const Tile<G> &t, const TileSmem &
                              : 0;
                 }
             }
-            val[x] = c;
+            lv[p - pb] = c;
+        }
+        for (int x = 0; x < P.iep_num; x++) {
+            const int p = P.iep_prefix[x];
+            const bool here = P.p_level[p] == k;
+            if (P.p_kind[p] == GAT_SET_COUNT) {
+                val[x] = here ? lv[p - pb] : (long long)S.sl[p];
+                continue;
+            }
+            const int32_t *ptr = here ? nb : S.sp[p];
+            int32_t len = here ? (int32_t)lv[p - pb] : S.sl[p];
+            const unsigned bm = P.iep_bound[x];
+            int32_t B = min_of(S, bm & ~kbit);
+            if (bm & kbit) B = min(B, cand);
+            if (B != kInf) len = lower_serial(ptr, len, B);
+            const unsigned m = P.iep_sub[x];
+            int h = 0;
+            for (int j = 0; j < P.basic; j++)
+                if ((m >> j) & 1u)
+                    h += contains(ptr, len, j == k ? cand : S.v[j], a.linear_below) ? 1 : 0;
+            val[x] = (long long)len - h;
         }
         unsigned long long local = 0, cur = 1;
         int last = -1;
@@ -598,7 +629,8 @@ __device__ __forceinline__ bool lane_worth(const TileSmem &S, const GatPlan &P, 
     const int32_t cnt = S.cnt[k];
     if (2 * cnt >= G) return true;
     int32_t fmax = 0;
-    for (int x = 0; x < P.iep_num; x++) fmax = max(fmax, S.sl[P.p_father[P.iep_prefix[x]]]);
+    for (int p = P.l_pbegin[k]; p < P.l_pbegin[k + 1]; p++)
+        if (P.p_kind[p] == GAT_SET_COUNT) fmax = max(fmax, S.sl[P.p_father[p]]);
     return cnt >= fmax;
 }
 

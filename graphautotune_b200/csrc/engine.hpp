@@ -32,6 +32,18 @@ cudaError_t build_hub_bitmaps(const int64_t *off, const int32_t *adj,
                               const int32_t *hubs, int32_t nhubs, int64_t words,
                               uint32_t *bitmaps, cudaStream_t stream);
 
+// lo_off[v] = sum over u < v of |{w in N(u) : w < u}| (V+1 entries), from a
+// device CSR with sorted rows (relabel.cu).
+cudaError_t lower_offsets_device(const int64_t *off, const int32_t *adj, int32_t V,
+                                 int64_t *lo_off, cudaStream_t stream);
+// Whether relabel_by_degree_device takes a graph of this size.
+bool relabel_fits_device(int32_t V, int64_t E);
+// The copy relabelled by decreasing degree (ties by id), rows sorted, built
+// from a device CSR into caller-allocated new_off (V+1) and new_adj (E).
+cudaError_t relabel_by_degree_device(const int64_t *off, const int32_t *adj, int32_t V,
+                                     int64_t E, int32_t max_degree, int64_t *new_off,
+                                     int32_t *new_adj, cudaStream_t stream);
+
 struct LaunchShape {
     int grid = 0;         // CTAs
     int block = 128;      // threads per CTA

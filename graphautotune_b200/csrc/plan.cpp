@@ -65,16 +65,15 @@ void assign_slots(GatPlan &pl) {
     pl.num_store = 0;
     for (int p = 0; p < pl.num_prefix; p++)
         if (pl.p_kind[p] == GAT_SET_STORE) pl.p_slot[p] = (int8_t)pl.num_store++;
-    // Lane-per-candidate last level: only counted sets at level basic-1,
-    // all of them fed to inclusion-exclusion, few slots.
+    // Lane-per-candidate last level: nothing at level basic-1 is stored
+    // (each set is a count with a father, or the candidate's own list), and
+    // at most 8 sets there and 8 IEP slots.
     const int k = pl.basic - 1;
-    bool ok = pl.basic >= 3 && pl.iep_num >= 1 && pl.iep_num <= 8;
+    bool ok = pl.basic >= 3 && pl.iep_num >= 1 && pl.iep_num <= 8 &&
+              pl.l_pbegin[k + 1] - pl.l_pbegin[k] <= 8;
     for (int p = pl.l_pbegin[k]; ok && p < pl.l_pbegin[k + 1]; p++)
-        ok = pl.p_kind[p] == GAT_SET_COUNT && pl.p_father[p] >= 0;
-    for (int x = 0; ok && x < pl.iep_num; x++) {
-        const int p = pl.iep_prefix[x];
-        ok = p >= pl.l_pbegin[k] && p < pl.l_pbegin[k + 1];
-    }
+        ok = (pl.p_kind[p] == GAT_SET_COUNT && pl.p_father[p] >= 0) ||
+             pl.p_kind[p] == GAT_SET_ALIAS;
     pl.lane_last = ok ? 1 : 0;
 }
 

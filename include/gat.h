@@ -182,6 +182,13 @@ int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
 /* Number of hub bitmaps on the given device copy (0: ids as given,
  * 1: degree-ordered). */
 int gat_graph_hubs(const gat_graph *g, int ordered_copy, int32_t *nhubs);
+/* Copies the degree-ordered device copy (uploaded with
+ * GAT_UPLOAD_DEGREE_ORDER) into host buffers of V+1 offsets and E
+ * neighbours.  Vertex r of that copy is the r-th vertex by decreasing degree,
+ * ties by id; exact counts by root range (gat_executor_count_range) name
+ * roots by these ids.  No reference counterpart: the reference counts on the
+ * ids as loaded. */
+int gat_graph_ordered_csr(const gat_graph *g, int64_t *offsets, int32_t *adj);
 void gat_graph_free(gat_graph *g);
 
 /* -------------------------------------------------------------- engine --

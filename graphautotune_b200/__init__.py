@@ -287,6 +287,7 @@ class CountResult:
     block: int
     tile: int
     scratch_bytes: int
+    launches: int = 1
 
 
 class Executor(_Handle):
@@ -310,7 +311,7 @@ class Executor(_Handle):
         if schedule.mode == MODE_REF_COMPAT and cnt >= 1 << 63:
             cnt -= 1 << 64
         return CountResult(cnt, st.kernel_ms, st.total_ms, st.raw_sum, st.divisor, st.tasks,
-                           st.balg_bytes, st.grid, st.block, st.tile, st.scratch_bytes)
+                           st.balg_bytes, st.grid, st.block, st.tile, st.scratch_bytes, st.launches)
 
     def count_range(self, graph: Graph, schedule: Schedule, root_begin: int, root_end: int,
                     stream: int | None = None) -> tuple[int, CountResult]:
@@ -322,7 +323,7 @@ class Executor(_Handle):
                                              root_begin, root_end, C.byref(raw), C.byref(st)))
         return raw.value, CountResult(raw.value, st.kernel_ms, st.total_ms, st.raw_sum,
                                       st.divisor, st.tasks, st.balg_bytes, st.grid, st.block,
-                                      st.tile, st.scratch_bytes)
+                                      st.tile, st.scratch_bytes, st.launches)
 
     def count_shard(self, graph: Graph, schedule: Schedule, shard: int, num_shards: int,
                     stream: int | None = None, balg: bool = False) -> tuple[int, CountResult]:
@@ -334,7 +335,7 @@ class Executor(_Handle):
                  shard, num_shards, C.byref(raw), C.byref(st)))
         return raw.value, CountResult(raw.value, st.kernel_ms, st.total_ms, st.raw_sum,
                                       st.divisor, st.tasks, st.balg_bytes, st.grid, st.block,
-                                      st.tile, st.scratch_bytes)
+                                      st.tile, st.scratch_bytes, st.launches)
 
     def perform_search(self, graph: Graph, schedule: Schedule) -> int:
         """long long Executor::perform_search(DeviceContext&)."""
@@ -365,7 +366,7 @@ class Batch(_Handle):
         st = gat_stats()
         check(lib().gat_batch_run(self._h, C.byref(st)))
         return CountResult(0, st.kernel_ms, st.total_ms, 0, 1, st.tasks, 0, st.grid, st.block,
-                           st.tile, st.scratch_bytes)
+                           st.tile, st.scratch_bytes, st.launches)
 
     def counts(self) -> list[int]:
         n = lib().gat_batch_size(self._h)

@@ -680,20 +680,37 @@ void gat_executor_free(gat_executor *e) { delete e; }
 
 namespace {
 
-// The exact 4-cycle count through the wedge-aggregation kernel: one V-word
-// counter row per resident tile, kept all-zero between launches.
-int run_c4(gat_executor *e, const DevGraphView &view, int64_t vb, int64_t ve,
-           LaunchShape shape, cudaStream_t strm, bool balg, bool ranged, uint64_t *count,
+// The exact 4-cycle count through the wedge-aggregation kernels: counter
+// rows for light tiles and heavy batches in scratch, kept all-zero between
+// launches.
+int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t vb,
+           int64_t ve, LaunchShape shape, cudaStream_t strm, bool balg, uint64_t *count,
            gat_stats *stats, std::chrono::steady_clock::time_point t0) {
     const int occ = c4_blocks_per_sm(shape.tile, shape.block, balg);
-    if (occ <= 0) return fail(GAT_ERR_CUDA, "4-cycle kernel does not fit on the device");
-    shape.grid = e->cfg.num_blocks > 0 ? e->cfg.num_blocks : e->sms * occ;
-    const int64_t stride = std::max<int64_t>(view.V, 1);
-    const int64_t per_block = int64_t(shape.block / shape.tile) * stride * 4;
+    const int hocc = c4_heavy_blocks_per_sm(balg);
+    if (occ <= 0 || hocc <= 0) return fail(GAT_ERR_CUDA, "4-cycle kernels do not fit on the device");
+    const int64_t V = std::max<int64_t>(view.V, 1);
+    // Heavy roots: the leading run of ids with degree >= kC4HeavyDegree (on a
+    // degree-ordered copy, exactly the vertices of that degree).
+    constexpr int64_t kC4HeavyDegree = 256;
+    int64_t H = 0;
+    while (H < view.V && dc.off_host[H + 1] - dc.off_host[H] >= kC4HeavyDegree) H++;
+    const int64_t cap = std::max<int64_t>(1024, V / 8);
     const int64_t budget = e->cfg.memory_budget > 0 ? e->cfg.memory_budget : (int64_t(16) << 30);
-    if (per_block > budget) return fail(GAT_ERR_MEMORY, "memory budget below one CTA's counters");
-    shape.grid = (int)std::min<int64_t>(shape.grid, budget / per_block);
-    const size_t need = size_t(per_block) * size_t(shape.grid);
+    const int64_t tiles_per_block = shape.block / shape.tile;
+    const int64_t row_bytes = V * 4;
+    // Half the budget for light tiles' rows, half for heavy batches.
+    int64_t light_grid = e->cfg.num_blocks > 0 ? e->cfg.num_blocks : (int64_t)e->sms * occ;
+    light_grid = std::min<int64_t>(light_grid, (budget / 2) / (tiles_per_block * row_bytes));
+    const int64_t heavy_row = row_bytes + cap * 4 + 4 + 8;
+    int64_t R = std::min<int64_t>(std::max<int64_t>(H, 1), (budget / 2) / heavy_row);
+    if (light_grid < 1 || R < 1)
+        return fail(GAT_ERR_MEMORY, "memory budget below the 4-cycle counters' minimum");
+    const int64_t light_bytes = light_grid * tiles_per_block * row_bytes;
+    const int64_t hrows_bytes = R * row_bytes;
+    const int64_t lists_bytes = R * cap * 4;
+    const int64_t lens_bytes = ((R * 4 + 255) / 256) * 256;
+    const size_t need = size_t(light_bytes + hrows_bytes + lists_bytes + lens_bytes + (R + 1) * 8);
     cudaError_t ce;
     if (need > e->scratch_bytes) {
         cudaFree(e->scratch);
@@ -709,9 +726,33 @@ int run_c4(gat_executor *e, const DevGraphView &view, int64_t vb, int64_t ve,
             return cuda_fail(ce, "counter clear");
         e->scratch_clean = true;
     }
+    unsigned char *base = reinterpret_cast<unsigned char *>(e->scratch);
+    C4Launch L;
+    L.g = view;
+    L.off_host = dc.off_host.data();
+    L.lo_host = dc.lo_host.data();
+    L.v_begin = vb;
+    L.v_end = ve;
+    L.heavy_end = H;
+    L.tile = shape.tile;
+    L.block = shape.block;
+    L.chunk = shape.chunk;
+    L.light_grid = (int)light_grid;
+    L.heavy_grid = e->sms * hocc;
+    L.ctr = e->ctr;
+    L.stride = V;
+    L.light_rows = reinterpret_cast<uint32_t *>(base);
+    L.heavy_rows = reinterpret_cast<uint32_t *>(base + light_bytes);
+    L.heavy_lists = reinterpret_cast<int32_t *>(base + light_bytes + hrows_bytes);
+    L.heavy_lens = reinterpret_cast<uint32_t *>(base + light_bytes + hrows_bytes + lists_bytes);
+    L.pref = reinterpret_cast<int64_t *>(base + light_bytes + hrows_bytes + lists_bytes +
+                                         lens_bytes);
+    L.rows_per_batch = R;
+    L.cap = cap;
+    L.stats = balg;
+    shape.grid = (int)light_grid;
     cudaEventRecord(e->ev0, strm);
-    ce = launch_c4(view, vb, ve, shape.tile, shape.grid, shape.block, shape.chunk, e->ctr,
-                   reinterpret_cast<uint32_t *>(e->scratch), stride, balg, strm);
+    ce = launch_c4(L, strm);
     if (ce != cudaSuccess) {
         e->scratch_clean = false;
         return cuda_fail(ce, "4-cycle launch");
@@ -736,11 +777,11 @@ int run_c4(gat_executor *e, const DevGraphView &view, int64_t vb, int64_t ve,
     st.grid = shape.grid;
     st.block = shape.block;
     st.tile = shape.tile;
-    st.launches = 1;
+    const int64_t hb = std::min(ve, H) > vb ? (std::min(ve, H) - vb + R - 1) / R : 0;
+    st.launches = (std::max(vb, H) < ve ? 1 : 0) + 3 * hb;
     st.scratch_bytes = (int64_t)need;
     st.total_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    (void)ranged;
     if (stats) *stats = st;
     return GAT_OK;
 }
@@ -820,14 +861,28 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
             vb = root_begin;
             ve = root_end;
         } else if (num_shards > 0) {
+            // Roots are split by their upper neighbours (the 4-cycle kernels'
+            // units): shard k takes the roots whose units start in its slice.
+            const auto &of = dc->off_host;
             const auto &lo = dc->lo_host;
-            vb = std::lower_bound(lo.begin(), lo.begin() + view.V, shape.task_begin) - lo.begin();
-            ve = shard + 1 == num_shards
-                     ? view.V
-                     : std::lower_bound(lo.begin(), lo.begin() + view.V, shape.task_end) -
-                           lo.begin();
+            auto first_root = [&](int64_t u) {
+                int64_t a = 0, n = view.V;
+                while (n > 0) {
+                    const int64_t h = n >> 1;
+                    if (of[a + h] - lo[a + h] < u) {
+                        a += h + 1;
+                        n -= h + 1;
+                    } else {
+                        n = h;
+                    }
+                }
+                return a;
+            };
+            const int64_t total = view.E - view.lo_total;
+            vb = first_root(total * shard / num_shards);
+            ve = shard + 1 == num_shards ? view.V : first_root(total * (shard + 1) / num_shards);
         }
-        return run_c4(e, view, vb, ve, shape, strm, balg, ranged, count, stats, t0);
+        return run_c4(e, view, *dc, vb, ve, shape, strm, balg, count, stats, t0);
     }
     int occ = blocks_per_sm(shape.tile, shape.block, balg);
     if (occ <= 0) return fail(GAT_ERR_CUDA, "kernel does not fit on the device");

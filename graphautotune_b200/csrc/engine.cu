@@ -28,6 +28,7 @@
 //
 // The kernel has no waits on other CTAs: the only inter-CTA interaction is
 // atomicAdd on the cursor and the totals.
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <cstring>
@@ -51,7 +52,6 @@ struct TileSmem {
     int32_t pad[2];
     const int32_t *src[GAT_MAX_VERTICES];
     const int32_t *sp[GAT_MAX_PREFIX];
-    long long val[GAT_MAX_PREFIX];
 };
 
 struct SearchArgs {
@@ -404,11 +404,15 @@ __device__ __forceinline__ void setup_level(const Tile<G> &t, TileSmem &S,
     t.sync();
 }
 
-// Inclusion-exclusion value of the current unit (valid on lane 0).
+// Inclusion-exclusion value of the current unit (valid on lane 0).  The
+// slot values live in lane 0's local memory (only lane 0 forms the terms),
+// which keeps the per-tile shared state small enough for 256 one-lane tiles
+// per CTA.
 template <int G>
 __device__ long long iep_value(const Tile<G> &t, TileSmem &S, const GatPlan &P,
                                int linear_below) {
     const int basic = P.basic;
+    long long vals[GAT_MAX_PREFIX];
     for (int x = 0; x < P.iep_num; x++) {
         const int p = P.iep_prefix[x];
         long long val;
@@ -426,13 +430,13 @@ __device__ long long iep_value(const Tile<G> &t, TileSmem &S, const GatPlan &P,
             hit = t.sum(hit);
             val = (long long)len - hit;
         }
-        if (t.lane == 0) S.val[x] = val;
+        if (t.lane == 0) vals[x] = val;
     }
     unsigned long long local = 0, cur = 1;
     if (t.lane == 0) {
         int last = -1;
         for (int g = 0; g < P.num_terms; g++) {
-            const unsigned long long v = (unsigned long long)S.val[P.t_slot[g]];
+            const unsigned long long v = (unsigned long long)vals[P.t_slot[g]];
             cur = (g == last + 1) ? v : cur * v;
             if (P.t_close[g]) {
                 last = g;
@@ -789,27 +793,63 @@ __global__ void __launch_bounds__(256)
 }
 
 // Exact 4-cycle count by wedge aggregation.  Every 4-cycle is counted once,
-// at its largest vertex v0 together with the vertex x opposite v0: its other
-// two vertices are common neighbours of v0 and x below v0.  So
-//   count = sum_{v0} sum_{x < v0} C(c(v0, x), 2),
-//   c(v0, x) = |{ v1 in N(v0) : v1 < v0, x in N(v1) }|   (x < v0 too).
-// A tile owns a range of v0 and a private counter row of V words in scratch
-// (all zero between vertices): pass 1 adds 1 to cnt[x] for every wedge
-// v0 - v1 - x with v1, x < v0; pass 2 walks the same wedges and takes each
-// counter with an atomic exchange against 0, so every x contributes its
-// C(c, 2) exactly once and the row is zero again afterwards.  The lower
-// neighbours of v0 are the prefix of its sorted row (lo_off), and each N(v1)
-// is cut at v0 by a lower bound.
+// at its smallest vertex v0 together with the vertex x opposite v0: its other
+// two vertices are common neighbours of v0 and x above v0.  So
+//   count = sum_{v0} sum_{x > v0} C(c(v0, x), 2),
+//   c(v0, x) = |{ v1 in N(v0) : v1 > v0, x in N(v1) }|   (x > v0 too).
+// On the degree-ordered copy (id 0 = largest degree) v0 is the cycle's
+// highest-degree vertex and v1 has degree <= deg(v0), so the wedges number
+// at most sum over edges of the smaller endpoint's degree, instead of
+// sum_v deg(v)^2 with the opposite orientation.
+//
+// The counters c(v0, .) are a V-word row that is all zero between roots:
+// pass 1 adds 1 to row[x] for every wedge v0 - v1 - x and records each x
+// the first time it is touched; pass 2 reads each recorded x once, adds
+// C(c, 2) and writes the word back to zero.
+//
+//  * Light roots (degree below the heavy threshold) take one tile each, a
+//    private row in scratch and a touched list in shared memory (if the list
+//    overflows, pass 2 walks the wedges again with an atomic exchange).
+//  * Heavy roots (the leading run of ids with large degree) are spread over
+//    the whole grid: a batch of R roots has R shared rows and touched lists
+//    in scratch, pass 1 hands out the (v0, v1) pairs of the batch through the
+//    cursor (in root order, so the rows in use at any time stay in L2), and
+//    a separate pass-2 launch drains the lists (or, for a row touched in
+//    more than `cap` places, scans the row) in fixed-size pieces.
+// Kernels of one count are ordered on the stream; none waits on another CTA.
+
+constexpr int kC4Piece = 4096;  // pass-2 entries per piece
+
+// First index i of the sorted a[0, n) with a[i] > x (one lane alone).
+__device__ __forceinline__ int upper_serial(const int32_t *a, int n, int32_t x) {
+    int lo = 0;
+    while (n > 0) {
+        const int h = n >> 1;
+        const bool right = a[lo + h] <= x;
+        lo = right ? lo + h + 1 : lo;
+        n = right ? n - h - 1 : h;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned long long pairs_of(unsigned c) {
+    return (unsigned long long)c * (c - 1) / 2;
+}
+
 template <int G, bool STATS>
 __global__ void __launch_bounds__(256)
-    c4_wedge_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+    c4_light_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
                     const int64_t *__restrict__ lo_off, int64_t v_begin, int64_t v_end,
                     int32_t chunk, DevCounters *ctr, uint32_t *cnt_all, int64_t cnt_stride) {
+    // 32 KB of touched lists per block whatever the tile width.
+    constexpr int kC4LightList = 32 * G;
+    __shared__ int32_t lists[256 / G][kC4LightList];
+    __shared__ int32_t lens[256 / G];
     const Tile<G> t;
     const int tiles_per_block = blockDim.x / G;
-    const int tile_in_block = threadIdx.x / G;
-    uint32_t *cnt =
-        cnt_all + ((int64_t)blockIdx.x * tiles_per_block + tile_in_block) * cnt_stride;
+    const int tib = threadIdx.x / G;
+    int32_t *list = lists[tib];
+    uint32_t *cnt = cnt_all + ((int64_t)blockIdx.x * tiles_per_block + tib) * cnt_stride;
     unsigned long long part = 0, bytes = 0;
     for (;;) {
         unsigned long long s = 0;
@@ -819,36 +859,243 @@ __global__ void __launch_bounds__(256)
         if (s >= (unsigned long long)v_end) break;
         const int64_t e = min((int64_t)s + chunk, v_end);
         for (int64_t v0 = (int64_t)s; v0 < e; v0++) {
-            const int32_t nlo = (int32_t)(lo_off[v0 + 1] - lo_off[v0]);
-            if (nlo < 2) continue;
-            const int32_t *l0 = adj + off[v0];
-            for (int i = 0; i < nlo; i++) {
-                const int32_t v1 = l0[i];
+            const int64_t o0 = off[v0];
+            const int32_t d0 = (int32_t)(off[v0 + 1] - o0);
+            const int32_t lo0 = (int32_t)(lo_off[v0 + 1] - lo_off[v0]);
+            if (d0 - lo0 < 2) continue;  // a cycle needs two neighbours above v0
+            if (t.lane == 0) lens[tib] = 0;
+            t.sync();
+            // pass 1: lane per upper neighbour v1
+            for (int i = lo0 + t.lane; i < d0; i += G) {
+                const int32_t v1 = adj[o0 + i];
                 const int64_t o1 = off[v1];
-                const int n1 = tile_bound<G, false>(t, adj + o1, (int)(off[v1 + 1] - o1),
-                                                    (int32_t)v0);
-                for (int k = t.lane; k < n1; k += G) atomicAdd(&cnt[adj[o1 + k]], 1u);
-                if (STATS && t.lane == 0) bytes += 8ull * (unsigned)n1;
+                const int32_t d1 = (int32_t)(off[v1 + 1] - o1);
+                const int32_t *n1 = adj + o1;
+                for (int k = upper_serial(n1, d1, (int32_t)v0); k < d1; k++) {
+                    const int32_t x = n1[k];
+                    if (atomicAdd(&cnt[x], 1u) == 0u) {
+                        const int p = atomicAdd(&lens[tib], 1);
+                        if (p < kC4LightList) list[p] = x;
+                    }
+                    if (STATS) bytes += 12;
+                }
             }
             t.sync();
-            for (int i = 0; i < nlo; i++) {
-                const int32_t v1 = l0[i];
-                const int64_t o1 = off[v1];
-                const int n1 = tile_bound<G, false>(t, adj + o1, (int)(off[v1 + 1] - o1),
-                                                    (int32_t)v0);
-                for (int k = t.lane; k < n1; k += G) {
-                    const unsigned long long c = atomicExch(&cnt[adj[o1 + k]], 0u);
-                    part += c * (c - 1) / 2;
+            const int L = lens[tib];
+            if (L <= kC4LightList) {
+                for (int j = t.lane; j < L; j += G) {
+                    const int32_t x = list[j];
+                    const uint32_t c = cnt[x];
+                    cnt[x] = 0u;
+                    part += pairs_of(c);
+                }
+                if (STATS) bytes += 8ull * (unsigned)L;
+            } else {
+                for (int i = lo0 + t.lane; i < d0; i += G) {
+                    const int32_t v1 = adj[o0 + i];
+                    const int64_t o1 = off[v1];
+                    const int32_t d1 = (int32_t)(off[v1 + 1] - o1);
+                    const int32_t *n1 = adj + o1;
+                    for (int k = upper_serial(n1, d1, (int32_t)v0); k < d1; k++)
+                        part += pairs_of(atomicExch(&cnt[n1[k]], 0u));
                 }
             }
             t.sync();
         }
     }
     part = t.sum(part);
+    if (STATS) bytes = t.sum(bytes);
     if (t.lane == 0) {
         atomicAdd(&ctr->result, part);
         if (STATS) atomicAdd(&ctr->bytes, bytes);
     }
+}
+
+// Pass 1 over heavy roots [r0, r1): the units are the pairs (v0, v1 > v0),
+// numbered by up(v) = off[v] - lo_off[v] (upper neighbours before v).  A warp
+// takes `chunk` consecutive units; each lane resolves its own, walks short
+// neighbour lists alone and hands long ones (>= 64 entries above v0) to the
+// whole warp.  A first touch is appended to the row's list while the list
+// length is at most cap, so a list that missed an entry always ends with a
+// length above cap (pass 2 then scans the row instead).
+template <bool STATS>
+__global__ void __launch_bounds__(256)
+    c4_heavy_pass1_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                          const int64_t *__restrict__ lo_off, int64_t r0, int64_t r1,
+                          int64_t u_begin, int64_t u_end, int32_t chunk, DevCounters *ctr,
+                          uint32_t *rows, int32_t *lists, uint32_t *lens, int64_t stride,
+                          int64_t cap) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long bytes = 0;
+    for (;;) {
+        unsigned long long s = 0;
+        if (lane == 0) s = (unsigned long long)u_begin + atomicAdd(&ctr->cursor, (unsigned long long)chunk);
+        s = __shfl_sync(0xffffffffu, s, 0);
+        if (s >= (unsigned long long)u_end) break;
+        const int64_t e = min((int64_t)s + chunk, u_end);
+        // root of the first unit: largest v in [r0, r1) with up(v) <= s + lane
+        int64_t v0 = r0;
+        {
+            const int64_t tu = (int64_t)s + lane;
+            int64_t lo = r0, n = r1 - r0;
+            while (n > 0) {
+                const int64_t h = n >> 1;
+                const int64_t m = lo + h;
+                const bool right = off[m + 1] - lo_off[m + 1] <= tu;
+                lo = right ? m + 1 : lo;
+                n = right ? n - h - 1 : h;
+            }
+            v0 = min(lo, r1 - 1);
+        }
+        for (int64_t base = (int64_t)s; base < e; base += 32) {
+            const int64_t tu = base + lane;
+            const bool live = tu < e;
+            int32_t s1 = 0, d1 = 0, row = 0;
+            int64_t o1 = 0;
+            if (live) {
+                while (off[v0 + 1] - lo_off[v0 + 1] <= tu) v0++;
+                const int64_t j = tu - (off[v0] - lo_off[v0]);
+                const int32_t lo0 = (int32_t)(lo_off[v0 + 1] - lo_off[v0]);
+                const int32_t v1 = adj[off[v0] + lo0 + j];
+                o1 = off[v1];
+                d1 = (int32_t)(off[v1 + 1] - o1);
+                s1 = upper_serial(adj + o1, d1, (int32_t)v0);
+                row = (int32_t)(v0 - r0);
+            }
+            const bool longl = live && d1 - s1 >= 64;
+            if (live && !longl) {
+                uint32_t *rw = rows + (int64_t)row * stride;
+                for (int k = s1; k < d1; k++) {
+                    const int32_t x = adj[o1 + k];
+                    if (atomicAdd(&rw[x], 1u) == 0u &&
+                        *(volatile uint32_t *)&lens[row] <= (uint32_t)cap) {
+                        const uint32_t p = atomicAdd(&lens[row], 1u);
+                        if (p < (uint32_t)cap) lists[(int64_t)row * cap + p] = x;
+                    }
+                }
+                if (STATS) bytes += 12ull * (unsigned)(d1 - s1);
+            }
+            unsigned big = __ballot_sync(0xffffffffu, longl);
+            while (big) {
+                const int src = __ffs(big) - 1;
+                big &= big - 1;
+                const int32_t bs = __shfl_sync(0xffffffffu, s1, src);
+                const int32_t bd = __shfl_sync(0xffffffffu, d1, src);
+                const int32_t br = __shfl_sync(0xffffffffu, row, src);
+                const int64_t bo = __shfl_sync(0xffffffffu, o1, src);
+                uint32_t *rw = rows + (int64_t)br * stride;
+                for (int k = bs + lane; k < bd; k += 32) {
+                    const int32_t x = adj[bo + k];
+                    if (atomicAdd(&rw[x], 1u) == 0u &&
+                        *(volatile uint32_t *)&lens[br] <= (uint32_t)cap) {
+                        const uint32_t p = atomicAdd(&lens[br], 1u);
+                        if (p < (uint32_t)cap) lists[(int64_t)br * cap + p] = x;
+                    }
+                }
+                if (STATS && lane == 0) bytes += 12ull * (unsigned)(bd - bs);
+            }
+        }
+    }
+    if (STATS) {
+        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+        if (lane == 0) atomicAdd(&ctr->bytes, bytes);
+    }
+}
+
+// Pass-2 work of each heavy row in pieces of kC4Piece entries: the touched
+// list, or the row's words above v0 when the list overflowed.  One block;
+// writes the exclusive prefix of piece counts to pref[0..R].
+__global__ void c4_heavy_pieces_kernel(const uint32_t *lens, int64_t r0, int32_t R, int64_t V,
+                                       int64_t cap, int64_t *pref) {
+    __shared__ int64_t part[1024];
+    const int per = (R + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per, e = min(R, b + per);
+    int64_t sum = 0;
+    for (int r = b; r < e; r++) {
+        const int64_t n = lens[r] <= (uint32_t)cap ? (int64_t)lens[r] : V - (r0 + r) - 1;
+        sum += (n + kC4Piece - 1) / kC4Piece;
+    }
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t acc = 0;
+        for (int i = 0; i < (int)blockDim.x; i++) {
+            const int64_t v = part[i];
+            part[i] = acc;
+            acc += v;
+        }
+        pref[R] = acc;
+    }
+    __syncthreads();
+    int64_t acc = part[threadIdx.x];
+    for (int r = b; r < e; r++) {
+        pref[r] = acc;
+        const int64_t n = lens[r] <= (uint32_t)cap ? (int64_t)lens[r] : V - (r0 + r) - 1;
+        acc += (n + kC4Piece - 1) / kC4Piece;
+    }
+}
+
+template <bool STATS>
+__global__ void __launch_bounds__(256)
+    c4_heavy_pass2_kernel(int64_t r0, int32_t R, int64_t V, uint32_t *rows,
+                          const int32_t *lists, const uint32_t *lens, int64_t stride,
+                          int64_t cap, const int64_t *pref, DevCounters *ctr) {
+    __shared__ int64_t piece;
+    __shared__ unsigned long long red[8];
+    unsigned long long part = 0, bytes = 0;
+    const int64_t total = pref[R];
+    for (;;) {
+        if (threadIdx.x == 0) piece = (int64_t)atomicAdd(&ctr->cursor, 1ull);
+        __syncthreads();
+        const int64_t q = piece;
+        __syncthreads();
+        if (q >= total) break;
+        int lo = 0, n = R;  // row: last r with pref[r] <= q
+        while (n > 0) {
+            const int h = n >> 1;
+            const bool right = pref[lo + h + 1] <= q;
+            lo = right ? lo + h + 1 : lo;
+            n = right ? n - h - 1 : h;
+        }
+        const int r = lo;
+        const int64_t first = (q - pref[r]) * kC4Piece;
+        uint32_t *rw = rows + (int64_t)r * stride;
+        const int64_t v0 = r0 + r;
+        if (lens[r] <= (uint32_t)cap) {
+            const int64_t end = min(first + kC4Piece, (int64_t)lens[r]);
+            const int32_t *ls = lists + (int64_t)r * cap;
+            for (int64_t j = first + threadIdx.x; j < end; j += blockDim.x) {
+                const int32_t x = ls[j];
+                const uint32_t c = rw[x];
+                rw[x] = 0u;
+                part += pairs_of(c);
+                if (STATS) bytes += 12;
+            }
+        } else {
+            const int64_t end = min(v0 + 1 + first + kC4Piece, V);
+            for (int64_t x = v0 + 1 + first + threadIdx.x; x < end; x += blockDim.x) {
+                const uint32_t c = rw[x];
+                if (c) {
+                    rw[x] = 0u;
+                    part += pairs_of(c);
+                }
+                if (STATS) bytes += 8;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (STATS) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) red[w] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long s = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += red[i];
+        atomicAdd(&ctr->result, s);
+    }
+    if (STATS && (threadIdx.x & 31) == 0) atomicAdd(&ctr->bytes, bytes);
 }
 
 template <int G, bool STATS>
@@ -977,10 +1224,21 @@ namespace {
 template <int G, bool STATS>
 int c4_occ(int block) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, c4_wedge_kernel<G, STATS>, block, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, c4_light_kernel<G, STATS>, block, 0) !=
         cudaSuccess)
         return 0;
     return n;
+}
+
+template <bool STATS>
+int c4_heavy_occ() {
+    int a = 0, b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, c4_heavy_pass1_kernel<STATS>, 256,
+                                                      0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, c4_heavy_pass2_kernel<STATS>, 256,
+                                                      0) != cudaSuccess)
+        return 0;
+    return min(a, b);
 }
 }  // namespace
 
@@ -998,31 +1256,70 @@ int c4_blocks_per_sm(int tile, int block, bool stats) {
 #undef GAT_C4O
 }
 
-cudaError_t launch_c4(const DevGraphView &g, int64_t v_begin, int64_t v_end, int tile,
-                      int grid, int block, int chunk, DevCounters *ctr, uint32_t *cnt,
-                      int64_t stride, bool stats, cudaStream_t st) {
+int c4_heavy_blocks_per_sm(bool stats) {
+    return stats ? c4_heavy_occ<true>() : c4_heavy_occ<false>();
+}
+
+cudaError_t launch_c4(const C4Launch &L, cudaStream_t st) {
+    const DevGraphView &g = L.g;
+    DevCounters *ctr = L.ctr;
     cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(DevCounters), st);
     if (e != cudaSuccess) return e;
-    const int ch = chunk > 0 ? chunk : 1;
+    const int ch = L.chunk > 0 ? L.chunk : 1;
+    const int64_t lb = std::max(L.v_begin, L.heavy_end), le = L.v_end;
+    if (lb < le) {
 #define GAT_C4L(G)                                                                             \
-    if (stats)                                                                                 \
-        c4_wedge_kernel<G, true><<<grid, block, 0, st>>>(g.off, g.adj, g.lo_off, v_begin,      \
-                                                         v_end, ch, ctr, cnt, stride);         \
+    if (L.stats)                                                                               \
+        c4_light_kernel<G, true><<<L.light_grid, L.block, 0, st>>>(                            \
+            g.off, g.adj, g.lo_off, lb, le, ch, ctr, L.light_rows, L.stride);                  \
     else                                                                                       \
-        c4_wedge_kernel<G, false><<<grid, block, 0, st>>>(g.off, g.adj, g.lo_off, v_begin,     \
-                                                          v_end, ch, ctr, cnt, stride);        \
+        c4_light_kernel<G, false><<<L.light_grid, L.block, 0, st>>>(                           \
+            g.off, g.adj, g.lo_off, lb, le, ch, ctr, L.light_rows, L.stride);                  \
     break
-    switch (tile) {
-        case 1: GAT_C4L(1);
-        case 2: GAT_C4L(2);
-        case 4: GAT_C4L(4);
-        case 8: GAT_C4L(8);
-        case 16: GAT_C4L(16);
-        case 32: GAT_C4L(32);
-        default: return cudaErrorInvalidValue;
-    }
+        switch (L.tile) {
+            case 1: GAT_C4L(1);
+            case 2: GAT_C4L(2);
+            case 4: GAT_C4L(4);
+            case 8: GAT_C4L(8);
+            case 16: GAT_C4L(16);
+            case 32: GAT_C4L(32);
+            default: return cudaErrorInvalidValue;
+        }
 #undef GAT_C4L
-    return cudaGetLastError();
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    const int64_t he = std::min(L.v_end, L.heavy_end);
+    auto up = [&](int64_t v) { return L.off_host[v] - L.lo_host[v]; };
+    for (int64_t r0 = L.v_begin; r0 < he; r0 += L.rows_per_batch) {
+        const int64_t r1 = std::min(r0 + L.rows_per_batch, he);
+        const int32_t R = (int32_t)(r1 - r0);
+        if ((e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess ||
+            (e = cudaMemsetAsync(L.heavy_lens, 0, sizeof(uint32_t) * R, st)) != cudaSuccess)
+            return e;
+        if (L.stats)
+            c4_heavy_pass1_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
+                g.off, g.adj, g.lo_off, r0, r1, up(r0), up(r1), 128, ctr, L.heavy_rows,
+                L.heavy_lists, L.heavy_lens, L.stride, L.cap);
+        else
+            c4_heavy_pass1_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
+                g.off, g.adj, g.lo_off, r0, r1, up(r0), up(r1), 128, ctr, L.heavy_rows,
+                L.heavy_lists, L.heavy_lens, L.stride, L.cap);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        c4_heavy_pieces_kernel<<<1, 1024, 0, st>>>(L.heavy_lens, r0, R, g.V, L.cap, L.pref);
+        if ((e = cudaGetLastError()) != cudaSuccess ||
+            (e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess)
+            return e;
+        if (L.stats)
+            c4_heavy_pass2_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
+                r0, R, g.V, L.heavy_rows, L.heavy_lists, L.heavy_lens, L.stride, L.cap, L.pref,
+                ctr);
+        else
+            c4_heavy_pass2_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
+                r0, R, g.V, L.heavy_rows, L.heavy_lists, L.heavy_lens, L.stride, L.cap, L.pref,
+                ctr);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 int batch_blocks_per_sm(int tile, int block) {

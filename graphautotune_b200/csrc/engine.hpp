@@ -65,14 +65,31 @@ struct DevCounters {
     unsigned long long error;
 };
 
-// Exact 4-cycle count by wedge aggregation over first vertices
-// [v_begin, v_end) (plans with special == GAT_SPECIAL_C4).  `cnt` holds one
-// V-word counter row per resident tile (grid x block/tile rows of `stride`
-// words); rows must be zero before the launch and are zero again after it.
+// Exact 4-cycle count by wedge aggregation over smallest vertices
+// [v_begin, v_end) (plans with special == GAT_SPECIAL_C4).  Roots below
+// heavy_end are spread over the grid in batches of rows_per_batch (shared
+// counter rows, touched lists of `cap` entries); the others take one tile
+// each with a private row (light_grid x block/tile rows).  Every row has
+// `stride` words, must be zero before the launch and is zero again after it.
+struct C4Launch {
+    DevGraphView g;
+    const int64_t *off_host = nullptr;  // host copies of off and lo_off
+    const int64_t *lo_host = nullptr;
+    int64_t v_begin = 0, v_end = 0, heavy_end = 0;
+    int tile = 32, block = 256, chunk = 8, light_grid = 0, heavy_grid = 0;
+    DevCounters *ctr = nullptr;
+    int64_t stride = 0;
+    uint32_t *light_rows = nullptr;
+    uint32_t *heavy_rows = nullptr;
+    int32_t *heavy_lists = nullptr;
+    uint32_t *heavy_lens = nullptr;
+    int64_t *pref = nullptr;
+    int64_t rows_per_batch = 1, cap = 0;
+    bool stats = false;
+};
 int c4_blocks_per_sm(int tile, int block, bool stats);
-cudaError_t launch_c4(const DevGraphView &g, int64_t v_begin, int64_t v_end, int tile,
-                      int grid, int block, int chunk, DevCounters *ctr, uint32_t *cnt,
-                      int64_t stride, bool stats, cudaStream_t st);
+int c4_heavy_blocks_per_sm(bool stats);
+cudaError_t launch_c4(const C4Launch &launch, cudaStream_t st);
 
 // Batched launches: host code fills an array of batch_job_bytes()-sized job
 // records (one per (plan, graph) pair), copies it and the chunk-aligned

@@ -140,15 +140,34 @@ def run_c4(args):
     tot_e = sum(gr.info()[1] for gr in graphs)
     emit(config="c4", graphs=len(graphs), patterns=len(pats), total_directed_edges=tot_e,
          setup_s=time.time() - t0, specs=specs)
-    # plain: one default-config launch per job, each synchronised
     ex = g.Executor(plain_config())
+    if args.estimate:
+        # Per-job cost from `slices` spread-out slices of each job's work
+        # queue, extrapolated (no full counts).
+        P, nsl = args.estimate, 4
+        total = 0.0
+        for gi, gr in enumerate(graphs):
+            per = []
+            for p in pats:
+                ms = sum(ex.count_shard(gr, scheds[p], i * P // nsl, P)[1].kernel_ms
+                         for i in range(nsl))
+                per.append(round(ms * P / nsl, 2))
+            total += sum(per)
+            emit(config="c4", estimate_graph=gi, spec=specs[gi], E=gr.info()[1],
+                 est_ms_per_pattern=per, est_ms=sum(per))
+        emit(config="c4", estimate_total_ms=total)
+        return
+    # plain: one default-config launch per job, each synchronised
     plain_counts, plain_ms, plain_wall = [], 0.0, 0.0
     t = time.perf_counter()
-    for gr in graphs:
+    for gi, gr in enumerate(graphs):
+        gms = 0.0
         for p in pats:
             r = ex.count(gr, scheds[p])
             plain_counts.append(r.count)
             plain_ms += r.kernel_ms
+            gms += r.kernel_ms
+        emit(config="c4", arm="plain", graph=gi, kernel_ms=gms)
     plain_wall = (time.perf_counter() - t) * 1e3
     emit(config="c4", arm="plain", launches=len(plain_counts), kernel_ms=plain_ms,
          wall_ms=plain_wall)
@@ -273,6 +292,8 @@ def main():
     ap.add_argument("--tune", type=int, default=0)
     ap.add_argument("--max-seconds", type=float, default=120.0)
     ap.add_argument("--parts", type=int, default=1024)
+    ap.add_argument("--estimate", type=int, default=0,
+                    help="c4: estimate every job from 4 slices of 1/N of its queue")
     ap.add_argument("--slices", type=int, default=8)
     args = ap.parse_args()
     import torch

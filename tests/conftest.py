@@ -82,3 +82,10 @@ def golden_graphs(gat):
     for p in sorted((GOLDEN / "graphs").glob("*.bin")):
         out[p.stem] = gat.Graph.load(str(p))
     return out
+
+
+@pytest.fixture(scope="session")
+def golden_ref_engine():
+    """Answers of the reference engine itself (its target/pm.cu built for
+    sm_100a and run on a B200) on the golden graphs."""
+    return json.loads((GOLDEN / "ref_engine_counts.json").read_text())

@@ -74,3 +74,21 @@ def test_ref_engine_flags_undefined_schedules(oracle, golden_schedules, golden_g
         if sd["ub_read"]:
             flagged += st in oracle.REF_UNDEFINED
     assert flagged > 0
+
+
+def test_oracle_ref_engine_equals_reference_binary(oracle, golden_schedules, golden_graphs,
+                                                   golden_ref_engine):
+    """The CPU restatement of the reference engine's per-unit rules gives the
+    reference engine's own answers (its CUDA build, run on a B200), for every
+    pattern up to 5 vertices on er60, k7 and rmat6 and the triangle on the
+    config-1 graph."""
+    checked = 0
+    for e in golden_ref_engine:
+        sd = golden_schedules[e["adj"]]
+        assert not sd.get("crash")
+        off, adj = golden_graphs[e["graph"]].csr()
+        st, got, _ = oracle.ref_engine(off, adj, sd)
+        assert st == 0, (e["graph"], e["pattern"])
+        assert got == e["ref_engine_answer"], (e["graph"], e["pattern"], got)
+        checked += 1
+    assert checked >= 140

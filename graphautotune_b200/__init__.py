@@ -355,7 +355,16 @@ class Batch(_Handle):
     def add(self, graph: Graph, schedule: Schedule) -> int:
         j = C.c_int32()
         check(lib().gat_batch_add(self._h, graph._h, schedule._h, C.byref(j)))
-        self._keep.append((graph, schedule))
+        self._keep.append((graph, schedule, False))
+        return j.value
+
+    def add_shard(self, graph: Graph, schedule: Schedule, shard: int, num_shards: int) -> int:
+        """One equal slice of the job's work queue; counts() reports the
+        slice's undivided raw total for it."""
+        j = C.c_int32()
+        check(lib().gat_batch_add_shard(self._h, graph._h, schedule._h, shard, num_shards,
+                                        C.byref(j)))
+        self._keep.append((graph, schedule, True))
         return j.value
 
     def prepare(self, config: Config | None = None, cuda_graph: bool = True) -> None:
@@ -373,8 +382,9 @@ class Batch(_Handle):
         arr = (C.c_uint64 * max(n, 1))()
         check(lib().gat_batch_counts(self._h, arr, n))
         out = []
-        for (g, s), v in zip(self._keep, arr[:n]):
-            out.append(v - (1 << 64) if s.mode == MODE_REF_COMPAT and v >= 1 << 63 else v)
+        for (g, s, sliced), v in zip(self._keep, arr[:n]):
+            signed = sliced or s.mode == MODE_REF_COMPAT  # raw slice totals can be < 0
+            out.append(v - (1 << 64) if signed and v >= 1 << 63 else v)
         return out
 
     def __len__(self) -> int:

@@ -118,6 +118,7 @@ _SIGS = {
                                                 C.POINTER(C.c_int64), C.POINTER(gat_stats)]),
     "gat_batch_create": (C.c_int, [C.POINTER(P)]),
     "gat_batch_add": (C.c_int, [P, P, P, C.POINTER(C.c_int32)]),
+    "gat_batch_add_shard": (C.c_int, [P, P, P, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "gat_batch_prepare": (C.c_int, [P, C.POINTER(gat_config), C.c_int]),
     "gat_batch_run": (C.c_int, [P, C.POINTER(gat_stats)]),
     "gat_batch_counts": (C.c_int, [P, C.POINTER(C.c_uint64), C.c_size_t]),

@@ -999,6 +999,7 @@ struct gat_batch {
     struct Job {
         gat_graph *g;
         const gat_schedule *s;
+        int shard = 0, num_shards = 0;  // num_shards > 0: one slice of the work queue
     };
     std::vector<Job> jobs;
     gat_config cfg{};
@@ -1074,6 +1075,19 @@ int gat_batch_add(gat_batch *b, gat_graph *g, const gat_schedule *s, int32_t *jo
     return GAT_OK;
 }
 
+int gat_batch_add_shard(gat_batch *b, gat_graph *g, const gat_schedule *s, int32_t shard,
+                        int32_t num_shards, int32_t *job_index) {
+    if (num_shards < 1 || shard < 0 || shard >= num_shards)
+        return fail(GAT_ERR_ARGUMENT, "shard index out of range");
+    int32_t idx = -1;
+    const int rc = gat_batch_add(b, g, s, &idx);
+    if (rc != GAT_OK) return rc;
+    b->jobs[size_t(idx)].shard = shard;
+    b->jobs[size_t(idx)].num_shards = num_shards;
+    if (job_index) *job_index = idx;
+    return GAT_OK;
+}
+
 int gat_batch_prepare(gat_batch *b, const gat_config *c, int use_cuda_graph) {
     if (!b) return fail(GAT_ERR_ARGUMENT, "null argument");
     if (b->jobs.empty()) return fail(GAT_ERR_STATE, "empty batch");
@@ -1121,7 +1135,8 @@ int gat_batch_prepare(gat_batch *b, const gat_config *c, int use_cuda_graph) {
         plans[j] = s->plan.plan;
         if (b->cfg.special_kernels == 0) plans[j].lane_last = 0;
         batch_fill_job(host_jobs.data() + j * jb, b->d_plans + j, plans[j], v,
-                       b->cfg.set_search_type, b->cfg.hub_bitmaps != 0);
+                       b->cfg.set_search_type, b->cfg.hub_bitmaps != 0, b->jobs[j].shard,
+                       b->jobs[j].num_shards);
         stride = std::max<int64_t>(stride, tile_scratch_ints(plans[j], v.max_degree));
         vstart[j] = vt;
         const int64_t n = batch_job_tasks(host_jobs.data() + j * jb);
@@ -1233,7 +1248,8 @@ int gat_batch_counts(const gat_batch *b, uint64_t *counts, size_t n) {
     if (b->raw.size() != b->jobs.size()) return fail(GAT_ERR_STATE, "batch has not run");
     if (n < b->jobs.size()) return fail(GAT_ERR_ARGUMENT, "output too small");
     for (size_t j = 0; j < b->jobs.size(); j++)
-        counts[j] = (uint64_t)(b->raw[j] / b->divisors[j]);
+        counts[j] = b->jobs[j].num_shards > 0 ? (uint64_t)b->raw[j]
+                                              : (uint64_t)(b->raw[j] / b->divisors[j]);
     return GAT_OK;
 }
 

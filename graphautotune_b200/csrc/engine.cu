@@ -73,8 +73,9 @@ struct SearchArgs {
     int64_t bitmap_words;
 };
 
-// One job of a batched launch: a plan on a graph (ctr, scratch, chunk and
-// task_begin of `args` are unused; the batch supplies them).
+// One job of a batched launch: a plan on a graph, over the level-1 units
+// [task_begin, num_tasks) (ctr, scratch and chunk of `args` are unused; the
+// batch supplies them).
 struct BatchJob {
     SearchArgs args;
 };
@@ -778,7 +779,7 @@ __global__ void __launch_bounds__(256)
         if (vs >= (unsigned long long)vtotal) break;
         const int j = tile_bound<G, true, int64_t>(t, vstart, num_jobs, (int64_t)vs) - 1;
         const BatchJob &job = jobs[j];
-        const int64_t start = (int64_t)vs - vstart[j];
+        const int64_t start = job.args.task_begin + ((int64_t)vs - vstart[j]);
         if (start >= job.args.num_tasks) continue;  // padding of the job's last chunk
         if (j != cur_job) {
             if (t.lane == 0 && cur_job >= 0 && acc) atomicAdd(&results[cur_job], acc);
@@ -1171,7 +1172,8 @@ size_t tile_smem_bytes() { return sizeof(TileSmem); }
 size_t batch_job_bytes() { return sizeof(BatchJob); }
 
 void batch_fill_job(void *dst, const GatPlan *d_plan, const GatPlan &h_plan,
-                    const DevGraphView &g, int linear_below, bool use_bitmaps) {
+                    const DevGraphView &g, int linear_below, bool use_bitmaps, int shard,
+                    int num_shards) {
     BatchJob j{};
     SearchArgs &a = j.args;
     a.plan = d_plan;
@@ -1180,8 +1182,9 @@ void batch_fill_job(void *dst, const GatPlan *d_plan, const GatPlan &h_plan,
     a.lo_off = g.lo_off;
     a.V = g.V;
     a.cap = g.max_degree > 0 ? g.max_degree : 1;
-    a.task_begin = 0;
-    a.num_tasks = h_plan.level1_bounded ? g.lo_total : g.E;
+    const int64_t total = h_plan.level1_bounded ? g.lo_total : g.E;
+    a.task_begin = num_shards > 0 ? total * shard / num_shards : 0;
+    a.num_tasks = num_shards > 0 ? total * (shard + 1) / num_shards : total;
     a.linear_below = linear_below;
     const bool hubs = use_bitmaps && g.bitmaps != nullptr && g.hub_slot != nullptr;
     a.hub_slot = hubs ? g.hub_slot : nullptr;
@@ -1191,7 +1194,8 @@ void batch_fill_job(void *dst, const GatPlan *d_plan, const GatPlan &h_plan,
 }
 
 int64_t batch_job_tasks(const void *job) {
-    return reinterpret_cast<const BatchJob *>(job)->args.num_tasks;
+    const SearchArgs &a = reinterpret_cast<const BatchJob *>(job)->args;
+    return a.num_tasks - a.task_begin;
 }
 
 namespace {

@@ -98,7 +98,8 @@ cudaError_t launch_c4(const C4Launch &launch, cudaStream_t st);
 // per job; cursor and results must be zero before the launch.
 size_t batch_job_bytes();
 void batch_fill_job(void *dst, const GatPlan *d_plan, const GatPlan &h_plan,
-                    const DevGraphView &g, int linear_below, bool use_bitmaps);
+                    const DevGraphView &g, int linear_below, bool use_bitmaps, int shard = 0,
+                    int num_shards = 0);
 int64_t batch_job_tasks(const void *job);
 int batch_blocks_per_sm(int tile, int block);
 cudaError_t launch_batch(const void *d_jobs, const int64_t *d_vstart, int32_t num_jobs,

@@ -180,8 +180,16 @@ def run_c4(args):
     if args.tune:
         from graphautotune_b200 import tuner
 
-        cfg, hist = tuner.tune_batch(b, budget=args.tune)
-        emit(config="c4", arm="tuner", history=hist)
+        # Launch shapes are timed on a sample batch: one slice of 1/P of every
+        # job's work queue, slices spread over the queues.
+        P = args.tune_parts
+        sample = g.Batch()
+        for j, (gr, p) in enumerate((gr, p) for gr in graphs for p in pats):
+            sample.add_shard(gr, scheds[p], (j * 7) % P, P)
+        t = time.perf_counter()
+        cfg, hist = tuner.tune_batch(sample, budget=args.tune)
+        emit(config="c4", arm="tuner", sample=f"1/{P} of every job", history=hist,
+             tuning_s=time.perf_counter() - t)
     b.prepare(cfg, cuda_graph=True)
     b.run()
     runs = []
@@ -292,6 +300,7 @@ def main():
     ap.add_argument("--tune", type=int, default=0)
     ap.add_argument("--max-seconds", type=float, default=120.0)
     ap.add_argument("--parts", type=int, default=1024)
+    ap.add_argument("--tune-parts", type=int, default=32)
     ap.add_argument("--estimate", type=int, default=0,
                     help="c4: estimate every job from 4 slices of 1/N of its queue")
     ap.add_argument("--slices", type=int, default=8)

@@ -259,6 +259,12 @@ typedef struct gat_batch gat_batch;
 int gat_batch_create(gat_batch **out);
 int gat_batch_add(gat_batch *b, gat_graph *g, const gat_schedule *s,
                   int32_t *job_index);
+/* As gat_batch_add, for one equal slice of the job's level-1 work queue
+ * (the slicing of gat_executor_count_shard).  Its entry in gat_batch_counts
+ * is the slice's undivided signed total.  Used to time launch shapes on a
+ * sample of every job. */
+int gat_batch_add_shard(gat_batch *b, gat_graph *g, const gat_schedule *s,
+                        int32_t shard, int32_t num_shards, int32_t *job_index);
 int gat_batch_prepare(gat_batch *b, const gat_config *c, int use_cuda_graph);
 int gat_batch_run(gat_batch *b, gat_stats *stats);
 int gat_batch_counts(const gat_batch *b, uint64_t *counts, size_t n);

@@ -41,3 +41,33 @@ def test_batch_equals_single_counts(gat):
                 r = b.run()
                 assert r.kernel_ms > 0 and r.tile == (shape.get("threads_per_warp") or 32)
                 assert b.counts() == want, (shape, cuda_graph)
+
+
+def test_sliced_jobs_sum_to_whole(gat):
+    """Jobs added as slices of their work queue (the autotuner's sample
+    batches) report raw totals that add up, over all slices, to the whole
+    job's raw total; the executor's shard counts agree slice by slice."""
+    graphs = [gat.Graph.rmat(11, 1 << 14, 0.57, 0.19, 0.19, 31),
+              gat.Graph.barabasi_albert(3000, 9, 32)]
+    pats = ["0111101111011110", "0100110110010110110010100", "0110010101100111010101110"]
+    P = 5
+    b = gat.Batch()
+    for gr in graphs:
+        for p in pats:
+            s = gat.Schedule(p, "exact")
+            for k in range(P):
+                b.add_shard(gr, s, k, P)
+    b.prepare(gat.Config.engine_default(), cuda_graph=True)
+    b.run()
+    raw = b.counts()
+    ex = gat.Executor(gat.Config.engine_default())
+    i = 0
+    for gr in graphs:
+        for p in pats:
+            s = gat.Schedule(p, "exact")
+            whole = ex.count(gr, s)
+            parts = raw[i:i + P]
+            assert parts == [ex.count_shard(gr, s, k, P)[0] for k in range(P)]
+            assert sum(parts) == whole.raw_sum
+            assert sum(parts) // whole.divisor == whole.count
+            i += P

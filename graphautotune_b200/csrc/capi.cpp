@@ -835,6 +835,10 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
     shape.tile = e->cfg.set_intersection_type == 1 ? 1 : e->cfg.threads_per_warp;
     shape.block = e->cfg.threads_per_block;
     shape.chunk = e->cfg.chunk > 0 ? e->cfg.chunk : 16;
+    // Two-level plans on the lane path give every lane its own level-1
+    // unit, so one grab holds `chunk` units per lane.
+    if (plan.basic == 2 && plan.lane_last && e->cfg.special_kernels != 0)
+        shape.chunk *= shape.tile;
     shape.linear_below = e->cfg.set_search_type;
     shape.use_bitmaps = e->cfg.hub_bitmaps != 0;
     const bool ranged = root_begin >= 0 || num_shards > 0;

@@ -490,19 +490,20 @@ __device__ __forceinline__ bool excluded(const TileSmem &S, unsigned ex, int k, 
 // set and each IEP value is formed exactly as level_sets and iep_value form
 // it for that candidate (same bounds, exclusions and bitmap-or-search
 // choice).  Returns the sum of the candidates' IEP values on every lane.
+// The candidates are src[i] for i in [i0, i1): the level's loop list (k >= 2),
+// or, at k = 1, the slice of N(v0) that holds the chunk's level-1 units.
 template <int G, bool STATS>
 __device__ unsigned long long lane_last_level(const Tile<G> &t, const TileSmem &S,
                                               const GatPlan &P, const SearchArgs &a, int k,
-                                              unsigned long long &bytes) {
-    const int32_t *src = S.src[k];
-    const int32_t cnt = S.cnt[k];
+                                              unsigned long long &bytes, const int32_t *src,
+                                              int i0, int i1) {
     const unsigned kbit = 1u << k;
     const int loop = P.l_loop[k];
     const int pb = P.l_pbegin[k], pe = P.l_pbegin[k + 1];
     unsigned long long sum = 0, by = 0;
     long long lv[8];   // level-k sets: count, or cut length of N(cand)
     long long val[8];  // IEP slots
-    for (int i = t.lane; i < cnt; i += G) {
+    for (int i = i0 + t.lane; i < i1; i += G) {
         const int32_t cand = src[i];
         bool hit = false;
         unsigned dm = P.l_distinct[k];
@@ -630,8 +631,8 @@ __device__ unsigned long long lane_last_level(const Tile<G> &t, const TileSmem &
 // outnumber the elements of the longest father list (the cooperative path
 // would then leave most lanes idle on every candidate).
 template <int G>
-__device__ __forceinline__ bool lane_worth(const TileSmem &S, const GatPlan &P, int k) {
-    const int32_t cnt = S.cnt[k];
+__device__ __forceinline__ bool lane_worth(const TileSmem &S, const GatPlan &P, int k,
+                                           int32_t cnt) {
     if (2 * cnt >= G) return true;
     int32_t fmax = 0;
     for (int p = P.l_pbegin[k]; p < P.l_pbegin[k + 1]; p++)
@@ -665,6 +666,18 @@ __device__ __forceinline__ void run_units(const Tile<G> &t, TileSmem &S, const G
             level_sets<G, STATS>(t, S, P, a, 0, v0, false, scratch, bytes);
             cur_v0 = v0;
         }
+        if (!ALL_ENTRIES && basic == 2 && P.lane_last) {
+            // Two-level plan: the lanes take this row's units of the chunk.
+            const int64_t row_end = min(end, task_off[v0 + 1]);
+            const int i0 = (int)(tk - task_off[v0]), i1 = (int)(row_end - task_off[v0]);
+            if (lane_worth<G>(S, P, 1, i1 - i0)) {
+                const unsigned long long r = lane_last_level<G, STATS>(
+                    t, S, P, a, 1, bytes, a.adj + a.off[v0], i0, i1);
+                if (t.lane == 0) acc += r;
+                tk = row_end - 1;
+                continue;
+            }
+        }
         if (t.lane == 0) S.v[1] = v1;
         t.sync();
         level_sets<G, STATS>(t, S, P, a, 1, v1, false, scratch, bytes,
@@ -676,8 +689,9 @@ __device__ __forceinline__ void run_units(const Tile<G> &t, TileSmem &S, const G
             continue;
         }
         setup_level(t, S, P, 2);
-        if (basic == 3 && P.lane_last && lane_worth<G>(S, P, 2)) {
-            const unsigned long long r = lane_last_level<G, STATS>(t, S, P, a, 2, bytes);
+        if (basic == 3 && P.lane_last && lane_worth<G>(S, P, 2, S.cnt[2])) {
+            const unsigned long long r =
+                lane_last_level<G, STATS>(t, S, P, a, 2, bytes, S.src[2], 0, S.cnt[2]);
             if (t.lane == 0) acc += r;
             continue;
         }
@@ -711,9 +725,9 @@ __device__ __forceinline__ void run_units(const Tile<G> &t, TileSmem &S, const G
                 continue;
             }
             setup_level(t, S, P, k + 1);
-            if (k + 1 == basic - 1 && P.lane_last && lane_worth<G>(S, P, k + 1)) {
-                const unsigned long long r =
-                    lane_last_level<G, STATS>(t, S, P, a, k + 1, bytes);
+            if (k + 1 == basic - 1 && P.lane_last && lane_worth<G>(S, P, k + 1, S.cnt[k + 1])) {
+                const unsigned long long r = lane_last_level<G, STATS>(
+                    t, S, P, a, k + 1, bytes, S.src[k + 1], 0, S.cnt[k + 1]);
                 if (t.lane == 0) acc += r;
                 continue;
             }

@@ -69,7 +69,7 @@ void assign_slots(GatPlan &pl) {
     // (each set is a count with a father, or the candidate's own list), and
     // at most 8 sets there and 8 IEP slots.
     const int k = pl.basic - 1;
-    bool ok = pl.basic >= 3 && pl.iep_num >= 1 && pl.iep_num <= 8 &&
+    bool ok = pl.basic >= 2 && pl.iep_num >= 1 && pl.iep_num <= 8 &&
               pl.l_pbegin[k + 1] - pl.l_pbegin[k] <= 8;
     for (int p = pl.l_pbegin[k]; ok && p < pl.l_pbegin[k + 1]; p++)
         ok = (pl.p_kind[p] == GAT_SET_COUNT && pl.p_father[p] >= 0) ||

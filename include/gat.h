@@ -114,7 +114,9 @@ typedef struct gat_config {
     int32_t threads_per_warp;      /* lanes per unit: 1,2,4,8,16,32 */
     int32_t max_regs;              /* accepted for compatibility; register
                                       use is fixed when the library is built */
-    int32_t chunk;                 /* level-1 units per work-queue grab */
+    int32_t chunk;                 /* level-1 units per work-queue grab (per
+                                      lane for two-level plans, whose lanes
+                                      take units one each) */
     int32_t hub_bitmaps;           /* 1: intersect against the graph's hub
                                       bitmaps where cheaper; 0: never */
     int64_t memory_budget;         /* bytes of scratch the executor may hold;

@@ -277,3 +277,26 @@ def test_four_cycle_heavy_batches_and_row_scans(gat, oracle):
                 assert r.launches > 3, r.launches  # heavy batches ran
         ex = _executor(gat, memory_budget=budget)
         assert sum(ex.count_shard(g, s, k, 5)[0] for k in range(5)) == want
+
+
+def test_full_size_workload_graph_against_oracle(gat):
+    """The bench's graph at full size (R-MAT 2^20, 2^24 samples, seed 2):
+    GPU reference-compatible 4-clique = the oracle's restatement of the
+    reference engine over the whole graph (tests/golden/c2_oracle.json,
+    made on the host by make_c2_oracle.py) = 4 x the GPU exact count."""
+    import json
+    from pathlib import Path
+
+    pins = json.loads((Path(__file__).parent / "golden" / "c2_oracle.json").read_text())
+    gspec = pins["graph"]
+    g = gat.Graph.rmat(gspec["scale"], gspec["samples"], *gspec["abc"], gspec["seed"])
+    assert g.info()[:2] == (gspec["V"], gspec["E"])
+    ex = gat.Executor(gat.Config.engine_default())
+    k4 = pins["k4"]
+    exact = ex.count(g, gat.Schedule(k4["pattern"], "exact")).count
+    ref = ex.count(g, gat.Schedule(k4["pattern"], "ref")).count
+    assert ref == k4["ref_engine_oracle"]
+    assert ref == 4 * exact
+    if "c4" in pins:
+        c4 = pins["c4"]
+        assert ex.count(g, gat.Schedule(c4["pattern"], "ref")).count == c4["ref_engine_oracle"]

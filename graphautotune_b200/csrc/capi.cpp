@@ -695,22 +695,22 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
     constexpr int64_t kC4HeavyDegree = 256;
     int64_t H = 0;
     while (H < view.V && dc.off_host[H + 1] - dc.off_host[H] >= kC4HeavyDegree) H++;
-    const int64_t cap = std::max<int64_t>(1024, V / 8);
+    const int64_t words = (V + 1023) / 1024;  // line bitmap: one bit per 32 counters
     const int64_t budget = e->cfg.memory_budget > 0 ? e->cfg.memory_budget : (int64_t(16) << 30);
     const int64_t tiles_per_block = shape.block / shape.tile;
     const int64_t row_bytes = V * 4;
-    // Half the budget for light tiles' rows, half for heavy batches.
+    // Half the budget for heavy batches; light tiles' rows get the other half,
+    // at most 4 GiB (with one-lane tiles every thread holds a row).
+    const int64_t light_budget = std::min<int64_t>(budget / 2, int64_t(4) << 30);
     int64_t light_grid = e->cfg.num_blocks > 0 ? e->cfg.num_blocks : (int64_t)e->sms * occ;
-    light_grid = std::min<int64_t>(light_grid, (budget / 2) / (tiles_per_block * row_bytes));
-    const int64_t heavy_row = row_bytes + cap * 4 + 4 + 8;
+    light_grid = std::min<int64_t>(light_grid, light_budget / (tiles_per_block * row_bytes));
+    const int64_t heavy_row = row_bytes + words * 4;
     int64_t R = std::min<int64_t>(std::max<int64_t>(H, 1), (budget / 2) / heavy_row);
     if (light_grid < 1 || R < 1)
         return fail(GAT_ERR_MEMORY, "memory budget below the 4-cycle counters' minimum");
     const int64_t light_bytes = light_grid * tiles_per_block * row_bytes;
     const int64_t hrows_bytes = R * row_bytes;
-    const int64_t lists_bytes = R * cap * 4;
-    const int64_t lens_bytes = ((R * 4 + 255) / 256) * 256;
-    const size_t need = size_t(light_bytes + hrows_bytes + lists_bytes + lens_bytes + (R + 1) * 8);
+    const size_t need = size_t(light_bytes + hrows_bytes + R * words * 4);
     cudaError_t ce;
     if (need > e->scratch_bytes) {
         cudaFree(e->scratch);
@@ -743,12 +743,9 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
     L.stride = V;
     L.light_rows = reinterpret_cast<uint32_t *>(base);
     L.heavy_rows = reinterpret_cast<uint32_t *>(base + light_bytes);
-    L.heavy_lists = reinterpret_cast<int32_t *>(base + light_bytes + hrows_bytes);
-    L.heavy_lens = reinterpret_cast<uint32_t *>(base + light_bytes + hrows_bytes + lists_bytes);
-    L.pref = reinterpret_cast<int64_t *>(base + light_bytes + hrows_bytes + lists_bytes +
-                                         lens_bytes);
+    L.heavy_bms = reinterpret_cast<uint32_t *>(base + light_bytes + hrows_bytes);
     L.rows_per_batch = R;
-    L.cap = cap;
+    L.words = words;
     L.stats = balg;
     shape.grid = (int)light_grid;
     cudaEventRecord(e->ev0, strm);
@@ -778,7 +775,7 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
     st.block = shape.block;
     st.tile = shape.tile;
     const int64_t hb = std::min(ve, H) > vb ? (std::min(ve, H) - vb + R - 1) / R : 0;
-    st.launches = (std::max(vb, H) < ve ? 1 : 0) + 3 * hb;
+    st.launches = (std::max(vb, H) < ve ? 1 : 0) + 2 * hb;
     st.scratch_bytes = (int64_t)need;
     st.total_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -818,22 +818,22 @@ __global__ void __launch_bounds__(256)
 // sum_v deg(v)^2 with the opposite orientation.
 //
 // The counters c(v0, .) are a V-word row that is all zero between roots:
-// pass 1 adds 1 to row[x] for every wedge v0 - v1 - x and records each x
-// the first time it is touched; pass 2 reads each recorded x once, adds
-// C(c, 2) and writes the word back to zero.
+// pass 1 adds 1 to row[x] for every wedge v0 - v1 - x and notes where it
+// wrote; pass 2 reads each noted counter once, adds C(c, 2) and writes the
+// word back to zero.
 //
 //  * Light roots (degree below the heavy threshold) take one tile each, a
-//    private row in scratch and a touched list in shared memory (if the list
-//    overflows, pass 2 walks the wedges again with an atomic exchange).
+//    private row in scratch and a list of first touches in shared memory (if
+//    the list overflows, pass 2 walks the wedges again with an atomic
+//    exchange).
 //  * Heavy roots (the leading run of ids with large degree) are spread over
-//    the whole grid: a batch of R roots has R shared rows and touched lists
-//    in scratch, pass 1 hands out the (v0, v1) pairs of the batch through the
-//    cursor (in root order, so the rows in use at any time stay in L2), and
-//    a separate pass-2 launch drains the lists (or, for a row touched in
-//    more than `cap` places, scans the row) in fixed-size pieces.
+//    the whole grid: a batch of R roots has R shared rows with line bitmaps
+//    in scratch; pass 1 hands out the (v0, v1) pairs of the batch through the
+//    cursor (in root order, so the rows in use at any time stay in L2) and
+//    increments counters with fire-and-forget atomics; a separate pass-2
+//    launch visits the marked lines.
 // Kernels of one count are ordered on the stream; none waits on another CTA.
 
-constexpr int kC4Piece = 4096;  // pass-2 entries per piece
 
 // First index i of the sorted a[0, n) with a[i] > x (one lane alone).
 __device__ __forceinline__ int upper_serial(const int32_t *a, int n, int32_t x) {
@@ -926,22 +926,45 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Heavy rows carry a line bitmap: bit (x >> 5) of the row's bitmap is set
+// when any counter of the 32-word line holding x was incremented.  Pass 1
+// increments counters with fire-and-forget atomics (no value comes back, so
+// no round trip stalls the warp) and sets line bits, batching the bits of one
+// bitmap word per lane and skipping the atomic when a plain read already
+// shows them; pass 2 visits only the marked lines.
+struct LineMarks {
+    uint32_t *bm = nullptr;
+    int64_t w = -1;
+    uint32_t bits = 0;
+    __device__ __forceinline__ void flush() {
+        if (bits && (bm[w] & bits) != bits) atomicOr(&bm[w], bits);
+        bits = 0;
+    }
+    __device__ __forceinline__ void mark(uint32_t *row_bm, int32_t x) {
+        const int64_t wi = x >> 10;
+        if (row_bm != bm || wi != w) {
+            if (bm) flush();
+            bm = row_bm;
+            w = wi;
+        }
+        bits |= 1u << ((x >> 5) & 31);
+    }
+};
+
 // Pass 1 over heavy roots [r0, r1): the units are the pairs (v0, v1 > v0),
 // numbered by up(v) = off[v] - lo_off[v] (upper neighbours before v).  A warp
 // takes `chunk` consecutive units; each lane resolves its own, walks short
 // neighbour lists alone and hands long ones (>= 64 entries above v0) to the
-// whole warp.  A first touch is appended to the row's list while the list
-// length is at most cap, so a list that missed an entry always ends with a
-// length above cap (pass 2 then scans the row instead).
+// whole warp.
 template <bool STATS>
 __global__ void __launch_bounds__(256)
     c4_heavy_pass1_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
                           const int64_t *__restrict__ lo_off, int64_t r0, int64_t r1,
                           int64_t u_begin, int64_t u_end, int32_t chunk, DevCounters *ctr,
-                          uint32_t *rows, int32_t *lists, uint32_t *lens, int64_t stride,
-                          int64_t cap) {
+                          uint32_t *rows, uint32_t *bms, int64_t stride, int64_t words) {
     const int lane = threadIdx.x & 31;
     unsigned long long bytes = 0;
+    LineMarks marks;
     for (;;) {
         unsigned long long s = 0;
         if (lane == 0) s = (unsigned long long)u_begin + atomicAdd(&ctr->cursor, (unsigned long long)chunk);
@@ -980,13 +1003,11 @@ __global__ void __launch_bounds__(256)
             const bool longl = live && d1 - s1 >= 64;
             if (live && !longl) {
                 uint32_t *rw = rows + (int64_t)row * stride;
+                uint32_t *bm = bms + (int64_t)row * words;
                 for (int k = s1; k < d1; k++) {
                     const int32_t x = adj[o1 + k];
-                    if (atomicAdd(&rw[x], 1u) == 0u &&
-                        *(volatile uint32_t *)&lens[row] <= (uint32_t)cap) {
-                        const uint32_t p = atomicAdd(&lens[row], 1u);
-                        if (p < (uint32_t)cap) lists[(int64_t)row * cap + p] = x;
-                    }
+                    atomicAdd(&rw[x], 1u);
+                    marks.mark(bm, x);
                 }
                 if (STATS) bytes += 12ull * (unsigned)(d1 - s1);
             }
@@ -999,100 +1020,65 @@ __global__ void __launch_bounds__(256)
                 const int32_t br = __shfl_sync(0xffffffffu, row, src);
                 const int64_t bo = __shfl_sync(0xffffffffu, o1, src);
                 uint32_t *rw = rows + (int64_t)br * stride;
+                uint32_t *bm = bms + (int64_t)br * words;
                 for (int k = bs + lane; k < bd; k += 32) {
                     const int32_t x = adj[bo + k];
-                    if (atomicAdd(&rw[x], 1u) == 0u &&
-                        *(volatile uint32_t *)&lens[br] <= (uint32_t)cap) {
-                        const uint32_t p = atomicAdd(&lens[br], 1u);
-                        if (p < (uint32_t)cap) lists[(int64_t)br * cap + p] = x;
-                    }
+                    atomicAdd(&rw[x], 1u);
+                    marks.mark(bm, x);
                 }
                 if (STATS && lane == 0) bytes += 12ull * (unsigned)(bd - bs);
             }
         }
     }
+    if (marks.bm) marks.flush();
     if (STATS) {
         for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
         if (lane == 0) atomicAdd(&ctr->bytes, bytes);
     }
 }
 
-// Pass-2 work of each heavy row in pieces of kC4Piece entries: the touched
-// list, or the row's words above v0 when the list overflowed.  One block;
-// writes the exclusive prefix of piece counts to pref[0..R].
-__global__ void c4_heavy_pieces_kernel(const uint32_t *lens, int64_t r0, int32_t R, int64_t V,
-                                       int64_t cap, int64_t *pref) {
-    __shared__ int64_t part[1024];
-    const int per = (R + blockDim.x - 1) / blockDim.x;
-    const int b = threadIdx.x * per, e = min(R, b + per);
-    int64_t sum = 0;
-    for (int r = b; r < e; r++) {
-        const int64_t n = lens[r] <= (uint32_t)cap ? (int64_t)lens[r] : V - (r0 + r) - 1;
-        sum += (n + kC4Piece - 1) / kC4Piece;
-    }
-    part[threadIdx.x] = sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int64_t acc = 0;
-        for (int i = 0; i < (int)blockDim.x; i++) {
-            const int64_t v = part[i];
-            part[i] = acc;
-            acc += v;
-        }
-        pref[R] = acc;
-    }
-    __syncthreads();
-    int64_t acc = part[threadIdx.x];
-    for (int r = b; r < e; r++) {
-        pref[r] = acc;
-        const int64_t n = lens[r] <= (uint32_t)cap ? (int64_t)lens[r] : V - (r0 + r) - 1;
-        acc += (n + kC4Piece - 1) / kC4Piece;
-    }
-}
-
+// Pass 2 over the R rows of a batch: a warp takes 32 bitmap words of one row
+// (1,024 lines), clears them, and for every marked line reads its 32 counters
+// in one coalesced access, adds C(c, 2) for each and writes the non-zero ones
+// back to zero.
 template <bool STATS>
 __global__ void __launch_bounds__(256)
-    c4_heavy_pass2_kernel(int64_t r0, int32_t R, int64_t V, uint32_t *rows,
-                          const int32_t *lists, const uint32_t *lens, int64_t stride,
-                          int64_t cap, const int64_t *pref, DevCounters *ctr) {
-    __shared__ int64_t piece;
+    c4_heavy_pass2_kernel(int32_t R, int64_t V, uint32_t *rows, uint32_t *bms, int64_t stride,
+                          int64_t words, DevCounters *ctr) {
     __shared__ unsigned long long red[8];
+    const int lane = threadIdx.x & 31;
+    const int64_t groups = (words + 31) / 32;
+    const int64_t total = (int64_t)R * groups;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long part = 0, bytes = 0;
-    const int64_t total = pref[R];
-    for (;;) {
-        if (threadIdx.x == 0) piece = (int64_t)atomicAdd(&ctr->cursor, 1ull);
-        __syncthreads();
-        const int64_t q = piece;
-        __syncthreads();
-        if (q >= total) break;
-        int lo = 0, n = R;  // row: last r with pref[r] <= q
-        while (n > 0) {
-            const int h = n >> 1;
-            const bool right = pref[lo + h + 1] <= q;
-            lo = right ? lo + h + 1 : lo;
-            n = right ? n - h - 1 : h;
+    for (int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < total;
+         gw += nwarps) {
+        const int64_t r = gw / groups, wg = (gw % groups) * 32;
+        uint32_t *bm = bms + r * words;
+        uint32_t *rw = rows + r * stride;
+        const int64_t wi = wg + lane;
+        uint32_t word = 0;
+        if (wi < words) {
+            word = bm[wi];
+            if (word) bm[wi] = 0u;
         }
-        const int r = lo;
-        const int64_t first = (q - pref[r]) * kC4Piece;
-        uint32_t *rw = rows + (int64_t)r * stride;
-        const int64_t v0 = r0 + r;
-        if (lens[r] <= (uint32_t)cap) {
-            const int64_t end = min(first + kC4Piece, (int64_t)lens[r]);
-            const int32_t *ls = lists + (int64_t)r * cap;
-            for (int64_t j = first + threadIdx.x; j < end; j += blockDim.x) {
-                const int32_t x = ls[j];
-                const uint32_t c = rw[x];
-                rw[x] = 0u;
-                part += pairs_of(c);
-                if (STATS) bytes += 12;
-            }
-        } else {
-            const int64_t end = min(v0 + 1 + first + kC4Piece, V);
-            for (int64_t x = v0 + 1 + first + threadIdx.x; x < end; x += blockDim.x) {
-                const uint32_t c = rw[x];
-                if (c) {
-                    rw[x] = 0u;
-                    part += pairs_of(c);
+        if (STATS) bytes += 4;
+        unsigned todo = __ballot_sync(0xffffffffu, word != 0u);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            uint32_t w = __shfl_sync(0xffffffffu, word, src);
+            const int64_t line0 = (wg + src) * 32;
+            while (w) {
+                const int b = __ffs(w) - 1;
+                w &= w - 1;
+                const int64_t x = (line0 + b) * 32 + lane;
+                if (x < V) {
+                    const uint32_t c = rw[x];
+                    if (c) {
+                        rw[x] = 0u;
+                        part += pairs_of(c);
+                    }
                 }
                 if (STATS) bytes += 8;
             }
@@ -1102,15 +1088,14 @@ __global__ void __launch_bounds__(256)
         part += __shfl_xor_sync(0xffffffffu, part, o);
         if (STATS) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
     }
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) red[w] = part;
+    if (lane == 0) red[threadIdx.x >> 5] = part;
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned long long s = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += red[i];
-        atomicAdd(&ctr->result, s);
+        unsigned long long t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += red[i];
+        atomicAdd(&ctr->result, t);
     }
-    if (STATS && (threadIdx.x & 31) == 0) atomicAdd(&ctr->bytes, bytes);
+    if (STATS && lane == 0) atomicAdd(&ctr->bytes, bytes);
 }
 
 template <int G, bool STATS>
@@ -1311,30 +1296,23 @@ cudaError_t launch_c4(const C4Launch &L, cudaStream_t st) {
     for (int64_t r0 = L.v_begin; r0 < he; r0 += L.rows_per_batch) {
         const int64_t r1 = std::min(r0 + L.rows_per_batch, he);
         const int32_t R = (int32_t)(r1 - r0);
-        if ((e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess ||
-            (e = cudaMemsetAsync(L.heavy_lens, 0, sizeof(uint32_t) * R, st)) != cudaSuccess)
+        if ((e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess)
             return e;
         if (L.stats)
             c4_heavy_pass1_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
                 g.off, g.adj, g.lo_off, r0, r1, up(r0), up(r1), 128, ctr, L.heavy_rows,
-                L.heavy_lists, L.heavy_lens, L.stride, L.cap);
+                L.heavy_bms, L.stride, L.words);
         else
             c4_heavy_pass1_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
                 g.off, g.adj, g.lo_off, r0, r1, up(r0), up(r1), 128, ctr, L.heavy_rows,
-                L.heavy_lists, L.heavy_lens, L.stride, L.cap);
+                L.heavy_bms, L.stride, L.words);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        c4_heavy_pieces_kernel<<<1, 1024, 0, st>>>(L.heavy_lens, r0, R, g.V, L.cap, L.pref);
-        if ((e = cudaGetLastError()) != cudaSuccess ||
-            (e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess)
-            return e;
         if (L.stats)
             c4_heavy_pass2_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
-                r0, R, g.V, L.heavy_rows, L.heavy_lists, L.heavy_lens, L.stride, L.cap, L.pref,
-                ctr);
+                R, g.V, L.heavy_rows, L.heavy_bms, L.stride, L.words, ctr);
         else
             c4_heavy_pass2_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
-                r0, R, g.V, L.heavy_rows, L.heavy_lists, L.heavy_lens, L.stride, L.cap, L.pref,
-                ctr);
+                R, g.V, L.heavy_rows, L.heavy_bms, L.stride, L.words, ctr);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;

@@ -68,9 +68,10 @@ struct DevCounters {
 // Exact 4-cycle count by wedge aggregation over smallest vertices
 // [v_begin, v_end) (plans with special == GAT_SPECIAL_C4).  Roots below
 // heavy_end are spread over the grid in batches of rows_per_batch (shared
-// counter rows, touched lists of `cap` entries); the others take one tile
-// each with a private row (light_grid x block/tile rows).  Every row has
-// `stride` words, must be zero before the launch and is zero again after it.
+// counter rows, each with a line bitmap of `words` words); the others take
+// one tile each with a private row (light_grid x block/tile rows).  Every
+// row has `stride` words; rows and bitmaps must be zero before the launch
+// and are zero again after it.
 struct C4Launch {
     DevGraphView g;
     const int64_t *off_host = nullptr;  // host copies of off and lo_off
@@ -81,10 +82,8 @@ struct C4Launch {
     int64_t stride = 0;
     uint32_t *light_rows = nullptr;
     uint32_t *heavy_rows = nullptr;
-    int32_t *heavy_lists = nullptr;
-    uint32_t *heavy_lens = nullptr;
-    int64_t *pref = nullptr;
-    int64_t rows_per_batch = 1, cap = 0;
+    uint32_t *heavy_bms = nullptr;
+    int64_t rows_per_batch = 1, words = 0;
     bool stats = false;
 };
 int c4_blocks_per_sm(int tile, int block, bool stats);

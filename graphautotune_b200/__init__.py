@@ -95,14 +95,27 @@ class Schedule(_Handle):
     _free = "gat_schedule_free"
 
     def __init__(self, pattern: Pattern | str, mode: str | int = "exact",
-                 stats_graph: "Graph | None" = None):
+                 stats_graph: "Graph | None" = None, variant: int = 0):
         super().__init__()
         if isinstance(pattern, str):
             pattern = Pattern(pattern)
         self.pattern = pattern
         self.mode = _MODES[mode]
+        self.variant = variant
         g = stats_graph._h if stats_graph is not None else None
-        check(lib().gat_schedule_build(pattern._h, self.mode, g, C.byref(self._h)))
+        check(lib().gat_schedule_build_variant(pattern._h, self.mode, g, variant,
+                                               C.byref(self._h)))
+
+    @staticmethod
+    def variants(pattern: Pattern | str, mode: str | int = "exact",
+                 stats_graph: "Graph | None" = None) -> int:
+        """How many distinct plans Schedule(..., variant=i) offers."""
+        if isinstance(pattern, str):
+            pattern = Pattern(pattern)
+        n = C.c_int32()
+        g = stats_graph._h if stats_graph is not None else None
+        check(lib().gat_schedule_variants(pattern._h, _MODES[mode], g, C.byref(n)))
+        return n.value
 
     def dump(self) -> dict:
         return json.loads(read_string(lib().gat_schedule_dump, self._h))

@@ -83,6 +83,8 @@ _SIGS = {
     "gat_pattern_free": (None, [P]),
     "gat_enumerate_patterns": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "gat_schedule_build": (C.c_int, [P, C.c_int, P, C.POINTER(P)]),
+    "gat_schedule_variants": (C.c_int, [P, C.c_int, P, C.POINTER(C.c_int32)]),
+    "gat_schedule_build_variant": (C.c_int, [P, C.c_int, P, C.c_int32, C.POINTER(P)]),
     "gat_schedule_mode": (C.c_int, [P]),
     "gat_schedule_dump": (C.c_int, [P, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "gat_schedule_plan": (C.c_int, [P, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),

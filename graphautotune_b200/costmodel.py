@@ -254,6 +254,20 @@ class TunerModel:
         return self.model.predict(X).tolist()
 
 
+class BatchTunerModel:
+    """Ranks launch shapes for a whole batch: the log of the summed predicted
+    times of its jobs, each job given by (graph features, plan features)."""
+
+    def __init__(self, model: CostModel, jobs: list[tuple[np.ndarray, np.ndarray]]):
+        self.model, self.jobs = model, jobs
+
+    def predict(self, xs: list[dict]) -> list[float]:
+        X = np.stack([features(gf, pf, d) for d in xs for gf, pf in self.jobs])
+        p = self.model.predict(X).reshape(len(xs), len(self.jobs)).astype(np.float64)
+        m = p.max(axis=1, keepdims=True)
+        return (m[:, 0] + np.log(np.exp(p - m).sum(axis=1))).tolist()
+
+
 def all_points() -> list[dict]:
     import itertools
 

@@ -168,10 +168,45 @@ int gat_enumerate_patterns(int n, char *buf, size_t cap, size_t *needed) {
 
 // ----------------------------------------------------------- schedule
 
+namespace {
+GraphStats stats_of(const gat_graph *g) {
+    GraphStats gs;
+    if (g && g->host.V > 0) {
+        gs.v = g->host.V;
+        gs.e = g->host.E / 2;
+        gs.tri = std::max<int64_t>(1, gs.e / 10);
+    }
+    return gs;
+}
+}  // namespace
+
+int gat_schedule_variants(const gat_pattern *p, int mode, const gat_graph *stats_graph,
+                          int32_t *count) {
+    if (!p || !count) return fail(GAT_ERR_ARGUMENT, "null argument");
+    if (mode != GAT_MODE_EXACT || p->p.n <= 2) {
+        *count = 1;
+        return GAT_OK;
+    }
+    PlanInfo pi;
+    std::string err;
+    int n = 0;
+    if (!plan_exact(p->p, stats_of(stats_graph), pi, &err, 0, &n))
+        return fail(GAT_ERR_PATTERN, err);
+    *count = n;
+    return GAT_OK;
+}
+
 int gat_schedule_build(const gat_pattern *p, int mode,
                        const gat_graph *stats_graph, gat_schedule **out) {
+    return gat_schedule_build_variant(p, mode, stats_graph, 0, out);
+}
+
+int gat_schedule_build_variant(const gat_pattern *p, int mode, const gat_graph *stats_graph,
+                               int32_t variant, gat_schedule **out) {
     if (!p || !out) return fail(GAT_ERR_ARGUMENT, "null argument");
     *out = nullptr;
+    if (variant < 0 || (variant > 0 && (mode != GAT_MODE_EXACT || p->p.n <= 2)))
+        return fail(GAT_ERR_ARGUMENT, "schedule variant out of range");
     if (mode != GAT_MODE_EXACT && mode != GAT_MODE_REF_COMPAT)
         return fail(GAT_ERR_ARGUMENT, "unknown mode");
     auto s = std::make_unique<gat_schedule>();
@@ -194,13 +229,11 @@ int gat_schedule_build(const gat_pattern *p, int mode,
             s->trivial = true;
             s->json = "{\"mode\":\"exact\",\"trivial\":true}";
         } else {
-            GraphStats gs;
-            if (stats_graph && stats_graph->host.V > 0) {
-                gs.v = stats_graph->host.V;
-                gs.e = stats_graph->host.E / 2;
-                gs.tri = std::max<int64_t>(1, gs.e / 10);
+            if (!plan_exact(p->p, stats_of(stats_graph), s->plan, &err, variant)) {
+                if (variant > 0 && err == "no such schedule variant")
+                    return fail(GAT_ERR_ARGUMENT, "schedule variant out of range");
+                return fail(GAT_ERR_PATTERN, err);
             }
-            if (!plan_exact(p->p, gs, s->plan, &err)) return fail(GAT_ERR_PATTERN, err);
             std::string perm, r;
             for (size_t i = 0; i < s->plan.perm.size(); i++)
                 perm += (i ? "," : "") + std::to_string(s->plan.perm[i]);

@@ -110,9 +110,13 @@ struct GraphStats {
     int64_t v = 5000, e = 1000000, tri = 10000;  // reference defaults
 };
 
-// Device plan for the exact (non-induced subgraph) count.
-bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out,
-                std::string *err);
+// Device plan for the exact (non-induced subgraph) count.  Candidate vertex
+// orders are ranked by the reference's cost formula; `variant` picks the
+// variant-th distinct plan in that ranking (0 = the cheapest), and
+// *num_variants (when given) receives how many distinct plans there are
+// (at most 16).
+bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out, std::string *err,
+                int variant = 0, int *num_variants = nullptr);
 
 // All connected patterns on n vertices, one per isomorphism class, each in
 // its lexicographically smallest adjacency string.

@@ -14,6 +14,7 @@
 //   divided by the (verified constant) number of surviving embeddings per
 //   subgraph.
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <numeric>
 #include <sstream>
@@ -207,8 +208,23 @@ bool plan_from_ref(const RefSchedule &s, PlanInfo &out, std::string *err) {
     return true;
 }
 
-bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out,
-                std::string *err) {
+namespace {
+struct ExactCand {
+    std::vector<int> perm;
+    Pattern q;
+    Pairs r;
+    int k = 0;
+    int64_t div = 1;
+    double cost = 0;
+};
+
+// Device plan of one candidate vertex order (see plan_exact).
+bool build_exact_plan(const Pattern &p, const ExactCand &best, int64_t aut, PlanInfo &out,
+                      std::string *err);
+}  // namespace
+
+bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out, std::string *err,
+                int variant, int *num_variants) {
     out = PlanInfo{};
     if (p.n < 3) {
         if (err) *err = "exact plans need at least 3 vertices";
@@ -227,17 +243,10 @@ bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out,
         if (pattern_valid(q)) kmax = std::max(kmax, iep_suffix_count(q));
     } while (std::next_permutation(perm.begin(), perm.end()));
 
-    struct Cand {
-        std::vector<int> perm;
-        Pattern q;
-        Pairs r;
-        int k = 0;
-        int64_t div = 1;
-        double cost = 0;
-    };
-    bool have = false;
-    Cand best;
-    for (int k = kmax; k >= 1 && !have; k--) {
+    // Every vertex order with the most IEP suffix vertices, cheapest first by
+    // the reference's cost formula (ties in permutation order).
+    std::vector<ExactCand> cands;
+    for (int k = kmax; k >= 1 && cands.empty(); k--) {
         std::iota(perm.begin(), perm.end(), 0);
         do {
             Pattern q = p.permuted(perm);
@@ -254,18 +263,46 @@ bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out,
                 if (div <= 0) continue;
                 used = rb;
             }
-            double cost = estimate_restrictions(q, used, (int)gs.v, gs.e,
-                                                gs.tri);
-            if (!have || cost < best.cost) {
-                have = true;
-                best = Cand{perm, q, used, k, div, cost};
-            }
+            double cost = estimate_restrictions(q, used, (int)gs.v, gs.e, gs.tri);
+            cands.push_back(ExactCand{perm, q, used, k, div, cost});
         } while (std::next_permutation(perm.begin(), perm.end()));
     }
-    if (!have) {
+    if (cands.empty()) {
         if (err) *err = "no exact schedule found";
         return false;
     }
+    std::stable_sort(cands.begin(), cands.end(),
+                     [](const ExactCand &x, const ExactCand &y) { return x.cost < y.cost; });
+    // Variant i = the i-th distinct device plan in that order (orders that
+    // differ by an automorphism give the same plan).
+    constexpr int kMaxVariants = 16;
+    std::vector<GatPlan> seen;
+    bool found = false;
+    for (const ExactCand &c : cands) {
+        PlanInfo pi;
+        if (!build_exact_plan(p, c, (int64_t)autp.size(), pi, err)) continue;
+        bool dup = false;
+        for (const GatPlan &g : seen) dup |= std::memcmp(&g, &pi.plan, sizeof(GatPlan)) == 0;
+        if (dup) continue;
+        seen.push_back(pi.plan);
+        if ((int)seen.size() - 1 == variant) {
+            out = std::move(pi);
+            found = true;
+        }
+        if ((found && !num_variants) || (int)seen.size() >= kMaxVariants) break;
+    }
+    if (num_variants) *num_variants = (int)seen.size();
+    if (!found) {
+        if (err && !seen.empty()) *err = "no such schedule variant";
+        return false;
+    }
+    return true;
+}
+
+namespace {
+bool build_exact_plan(const Pattern &p, const ExactCand &best, int64_t aut, PlanInfo &out,
+                      std::string *err) {
+    out = PlanInfo{};
     Structure st;
     if (!build_structure(best.q, best.k, st, err)) return false;
     if (!check_sizes(st, err)) return false;
@@ -363,7 +400,7 @@ bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out,
     assign_slots(pl);
     out.perm = best.perm;
     out.restrictions = best.r;
-    out.aut = (int64_t)autp.size();
+    out.aut = aut;
     std::ostringstream o;
     o << "exact plan: suffix " << best.k << ", divisor " << best.div
       << ", cost " << best.cost;
@@ -377,5 +414,6 @@ bool plan_exact(const Pattern &p, const GraphStats &gs, PlanInfo &out,
     }
     return true;
 }
+}  // namespace
 
 }  // namespace gat

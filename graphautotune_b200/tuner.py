@@ -172,6 +172,23 @@ def propose(model, hist: History, batch: int, rng: random.Random, n_iter: int = 
     return [p for _, p in sorted(pool.values(), key=lambda t: t[0])[:batch]]
 
 
+def pick_schedule(ex: "g.Executor", graph: "g.Graph", pattern: str, parts: int = 256,
+                  slices: int = 4, stats_graph=None):
+    """Data-aware schedule choice: times every distinct exact plan of the
+    best-ranked vertex orders on `slices` spread slices (shards i*P/S of P)
+    of its work queue and returns (fastest schedule, [(variant, ms)])."""
+    n = g.Schedule.variants(pattern, "exact", stats_graph)
+    timings, best = [], None
+    for v in range(n):
+        s = g.Schedule(pattern, "exact", stats_graph, variant=v)
+        ms = sum(ex.count_shard(graph, s, i * parts // slices, parts)[1].kernel_ms
+                 for i in range(slices))
+        timings.append((v, ms))
+        if best is None or ms < best[1]:
+            best = (s, ms)
+    return best[0], timings
+
+
 def measure_batch(b: "g.Batch", d: dict, reps: int = 2) -> float:
     b.prepare(to_config(d), cuda_graph=True)
     b.run()

@@ -83,6 +83,18 @@ int gat_enumerate_patterns(int n, char *buf, size_t cap, size_t *needed);
  *     (core/schedule.hpp:909-910). */
 int gat_schedule_build(const gat_pattern *p, int mode,
                        const gat_graph *stats_graph, gat_schedule **out);
+/* Data-aware schedule choice (no reference counterpart: the reference keeps
+ * the first schedule its cost formula ranks best, core/schedule.hpp:878-926).
+ * For GAT_MODE_EXACT, *count receives the number of distinct exact plans
+ * among the best-ranked vertex orders (at most 16; 1 for other modes), and
+ * gat_schedule_build_variant builds plan `variant` of them (0 = the one
+ * gat_schedule_build returns).  Every variant counts the same subgraphs; a
+ * caller times them on a slice of the work queue and keeps the fastest. */
+int gat_schedule_variants(const gat_pattern *p, int mode,
+                          const gat_graph *stats_graph, int32_t *count);
+int gat_schedule_build_variant(const gat_pattern *p, int mode,
+                               const gat_graph *stats_graph, int32_t variant,
+                               gat_schedule **out);
 int gat_schedule_mode(const gat_schedule *s);
 /* JSON with the fields of Schedule::output() (core/schedule.hpp:752-784)
  * plus the chosen permutation and restrictions.  *needed = bytes incl NUL. */

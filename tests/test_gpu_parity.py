@@ -297,3 +297,26 @@ def test_full_size_workload_graph_against_oracle(gat):
     if "c4" in pins:
         c4 = pins["c4"]
         assert ex.count(g, gat.Schedule(c4["pattern"], "ref")).count == c4["ref_engine_oracle"]
+
+
+def test_schedule_variants_count_the_same(gat, oracle):
+    """Every exact plan variant gives the same count on the GPU (and the
+    oracle's on a small graph); the slice-timed pick returns one of them."""
+    from graphautotune_b200 import tuner
+
+    ex = _executor(gat, **CONFIGS[0])
+    small = gat.Graph.barabasi_albert(800, 4, 17)
+    big = gat.Graph.rmat(13, 1 << 16, 0.57, 0.19, 0.19, 18)
+    off, adj = small.csr()
+    for p in ("0100110110010110110010100", "0001100101010101010011000",
+              "011000101100110011000110001010001100"):
+        n = gat.Schedule.variants(p)
+        want_small = oracle.exact_count(off, adj, p)
+        counts = set()
+        for v in range(n):
+            s = gat.Schedule(p, "exact", variant=v)
+            assert ex.count(small, s).count == want_small, (p, v)
+            counts.add(ex.count(big, s).count)
+        assert len(counts) == 1, (p, counts)
+        best, timings = tuner.pick_schedule(ex, big, p, parts=16, slices=2)
+        assert len(timings) == n and ex.count(big, best).count in counts

@@ -169,3 +169,30 @@ def test_lane_last_flag(gat):
         assert P.lane_last == int(ok), p
         flagged += P.lane_last
     assert flagged > 20
+
+
+def test_every_schedule_variant_is_exact(gat, oracle, golden_graphs):
+    """Data-aware schedule choice may run any of the distinct exact plans of
+    the best-ranked vertex orders: each of them, interpreted on the CPU,
+    gives the oracle's count."""
+    pats = ["0100110110010110110010100", "0001100101010101010011000",
+            "0110010101100111010101110", "0001100111010111110111110",
+            "011000101100110011000110001010001100"]
+    checked = 0
+    for name in ("er60", "ba60"):
+        off, adj = golden_graphs[name].csr()
+        for p in pats:
+            n = gat.Schedule.variants(p)
+            assert 1 <= n <= 16
+            want = oracle.exact_count(off, adj, p)
+            plans = set()
+            for v in range(n):
+                raw_plan = gat.Schedule(p, "exact", variant=v).plan_bytes()
+                plans.add(raw_plan)
+                raw, div = plan_model.run(plan_model.parse(raw_plan), off, adj)
+                assert raw % div == 0 and raw // div == want, (name, p, v)
+                checked += 1
+            assert len(plans) == n  # variants are distinct plans
+            with pytest.raises(gat.GatError):
+                gat.Schedule(p, "exact", variant=n)
+    assert checked > 20

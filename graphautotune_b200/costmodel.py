@@ -180,8 +180,9 @@ def training_graphs(count: int, seed0: int = 1000) -> list[dict]:
 
 
 def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
-            log=None) -> tuple[np.ndarray, np.ndarray]:
-    """Times `runs` random (graph, pattern, configuration) counts."""
+            log=None, max_seconds: float = 0.0) -> tuple[np.ndarray, np.ndarray]:
+    """Times `runs` random (graph, pattern, configuration) counts (fewer if
+    `max_seconds` > 0 runs out first)."""
     from graphautotune_b200.experiments import make_graph
 
     rng = random.Random(seed)
@@ -197,7 +198,7 @@ def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
     execs: dict[str, g.Executor] = {}
     slow: set = set()
     t0 = time.time()
-    while len(X) < runs:
+    while len(X) < runs and not (max_seconds > 0 and time.time() - t0 > max_seconds):
         gi, si = rng.randrange(len(glist)), rng.randrange(len(scheds))
         if (gi, si) in slow:
             continue
@@ -294,6 +295,7 @@ def main():
     c.add_argument("--runs", type=int, default=20000)
     c.add_argument("--out", default="costmodel_data.npz")
     c.add_argument("--seed", type=int, default=0)
+    c.add_argument("--max-seconds", type=float, default=0.0)
     t = sub.add_parser("train")
     t.add_argument("data")
     t.add_argument("--out", default="costmodel.npz")
@@ -307,7 +309,8 @@ def main():
 
     torch.cuda.set_device(0)
     if a.cmd == "collect":
-        X, T = collect(a.runs, a.seed, log=lambda s: print(s, file=sys.stderr, flush=True))
+        X, T = collect(a.runs, a.seed, log=lambda s: print(s, file=sys.stderr, flush=True),
+                       max_seconds=a.max_seconds)
         np.savez(a.out, X=X, T=T)
         print(json.dumps({"runs": len(X), "features": X.shape[1], "out": a.out}))
     elif a.cmd == "train":

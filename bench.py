@@ -127,11 +127,15 @@ def measured_peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def profile_traffic() -> float | None:
+def profile_traffic(pattern: str) -> float | None:
+    """DRAM bytes (read + write) of one full count of `pattern` on the
+    workload graph, from the ncu capture summarised in profiles/."""
     p = ROOT / "profiles" / "traffic.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get(WORKLOAD["name"])
+            d = json.loads(p.read_text()).get(WORKLOAD["name"], {})
+            v = d.get(pattern) if isinstance(d, dict) else None
+            return None if v is None else float(v["bytes_per_count"])
         except Exception:
             return None
     return None
@@ -432,7 +436,7 @@ def run_ours(args):
             "wall_ms_per_step": wall * 1000 / args.steps,
             "setup": {"graph_build_s": t_gen, "upload_s": t_up},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": profile_traffic(),
+                         "frac": achieved / peak, "traffic": profile_traffic(dom),
                          "kernel": ("4-cycle wedge kernels (one count)" if dom == "c4"
                                     else f"search_kernel ({dom})"),
                          "balg_bytes_per_launch": balg,

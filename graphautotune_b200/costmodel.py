@@ -161,16 +161,20 @@ def features(gf: np.ndarray, pf: np.ndarray, d: dict) -> np.ndarray:
 
 # ---------------------------------------------------------------- data
 
-def training_graphs(count: int, seed0: int = 1000) -> list[dict]:
-    """Graphs like configuration 4's, smaller: n log-uniform in [2^10, 2^16],
-    half R-MAT (average degree 16), half Barabasi-Albert (m in 4..32)."""
+EXEC_BUDGET = 256 << 20  # scratch budget of the executors that gather timings
+
+
+def training_graphs(count: int, seed0: int = 1000, max_log2: int = 16) -> list[dict]:
+    """Graphs like configuration 4's, smaller: n log-uniform in
+    [2^10, 2^max_log2], half R-MAT (average degree 16), half
+    Barabasi-Albert (m in 4..32)."""
     from graphautotune_b200.experiments import splitmix
 
     specs = []
     for i in range(count):
         s = seed0 + i
         u = (splitmix(s) >> 11) / float(1 << 53)
-        n = int(2 ** (10 + 6 * u))
+        n = int(2 ** (10 + (max_log2 - 10) * u))
         if i % 2 == 0:
             scale = max(1, int(round(math.log2(n))))
             specs.append({"seed": s, "kind": "rmat", "scale": scale, "samples": 8 << scale})
@@ -195,7 +199,11 @@ def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
     scheds = [g.Schedule(p, "exact") for p in pats]
     pfs = [plan_features(s) for s in scheds]
     X, T = [], []
-    execs: dict[str, g.Executor] = {}
+    # a few executors at a time (each keeps its scratch), with a modest
+    # memory budget: thousands of random configurations are visited
+    from collections import OrderedDict
+
+    execs: "OrderedDict[str, g.Executor]" = OrderedDict()
     slow: set = set()
     t0 = time.time()
     while len(X) < runs and not (max_seconds > 0 and time.time() - t0 > max_seconds):
@@ -205,7 +213,12 @@ def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
         d = tuner.random_point(rng)
         key = tuner.fingerprint(d)
         if key not in execs:
-            execs[key] = g.Executor(tuner.to_config(d))
+            cfg = tuner.to_config(d)
+            cfg.memory_budget = EXEC_BUDGET
+            execs[key] = g.Executor(cfg)
+            if len(execs) > 8:
+                execs.popitem(last=False)
+        execs.move_to_end(key)
         gr, gf = glist[gi]
         r = execs[key].count(gr, scheds[si])
         if r.kernel_ms > max_ms:

@@ -1255,7 +1255,9 @@ int gat_batch_run(gat_batch *b, gat_stats *stats) {
     b->raw.assign(J, 0);
     for (size_t j = 0; j < J; j++) {
         b->raw[j] = (int64_t)b->h_results[j];
-        if (b->divisors[j] <= 0 || b->raw[j] % b->divisors[j] != 0)
+        // a whole job's total is a multiple of its divisor; a slice's need not be
+        if (b->jobs[j].num_shards == 0 &&
+            (b->divisors[j] <= 0 || b->raw[j] % b->divisors[j] != 0))
             return fail(GAT_ERR_DEVICE, "job total is not a multiple of its plan divisor");
     }
     if (stats) {

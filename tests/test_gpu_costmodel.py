@@ -53,7 +53,7 @@ def test_trained_model_beats_choosing_without_it(gat):
     from graphautotune_b200 import costmodel, tuner
     from graphautotune_b200.experiments import make_graph
 
-    specs = costmodel.training_graphs(10, seed0=5000)
+    specs = costmodel.training_graphs(10, seed0=5000, max_log2=13)
     graphs = []
     for sp in specs:
         gr = make_graph(sp)
@@ -69,7 +69,10 @@ def test_trained_model_beats_choosing_without_it(gat):
         d = tuner.random_point(rng)
         if all(tuner.fingerprint(d) != tuner.fingerprint(c) for c in cands):
             cands.append(d)
-    execs = [gat.Executor(tuner.to_config(d)) for d in cands]
+    cfgs = [tuner.to_config(d) for d in cands]
+    for c in cfgs:
+        c.memory_budget = costmodel.EXEC_BUDGET
+    execs = [gat.Executor(c) for c in cfgs]
     groups = []  # (graph index, X rows, measured ms)
     for gi, (gr, gf) in enumerate(graphs):
         for si, s in enumerate(scheds):

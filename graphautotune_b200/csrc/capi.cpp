@@ -743,7 +743,20 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
         return fail(GAT_ERR_MEMORY, "memory budget below the 4-cycle counters' minimum");
     const int64_t light_bytes = light_grid * tiles_per_block * row_bytes;
     const int64_t hrows_bytes = R * row_bytes;
-    const size_t need = size_t(light_bytes + hrows_bytes + R * words * 4);
+    const int64_t bms_bytes = ((R * words * 4 + 255) / 256) * 256;
+    // the largest number of (root, upper neighbour) units in one heavy batch
+    int64_t max_units = 0;
+    {
+        auto up = [&](int64_t v) { return dc.off_host[v] - dc.lo_host[v]; };
+        const int64_t he = std::min(ve, H);
+        for (int64_t r0 = vb; r0 < he; r0 += R)
+            max_units = std::max(max_units, up(std::min(r0 + R, he)) - up(r0));
+    }
+    const int64_t np_bytes = (((max_units + 1) * 4 + 255) / 256) * 256;
+    const int64_t pref_bytes = (((max_units + 1) * 8 + 255) / 256) * 256;
+    const int64_t temp_bytes = (((int64_t)c4_scan_temp_bytes(max_units + 1) + 255) / 256) * 256;
+    const size_t need = size_t(light_bytes + hrows_bytes + bms_bytes + np_bytes + pref_bytes +
+                               temp_bytes);
     cudaError_t ce;
     if (need > e->scratch_bytes) {
         cudaFree(e->scratch);
@@ -777,6 +790,11 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
     L.light_rows = reinterpret_cast<uint32_t *>(base);
     L.heavy_rows = reinterpret_cast<uint32_t *>(base + light_bytes);
     L.heavy_bms = reinterpret_cast<uint32_t *>(base + light_bytes + hrows_bytes);
+    unsigned char *tail = base + light_bytes + hrows_bytes + bms_bytes;
+    L.npieces = reinterpret_cast<int32_t *>(tail);
+    L.pieces_pref = reinterpret_cast<int64_t *>(tail + np_bytes);
+    L.scan_temp = tail + np_bytes + pref_bytes;
+    L.scan_temp_bytes = (size_t)temp_bytes;
     L.rows_per_batch = R;
     L.words = words;
     L.stats = balg;
@@ -808,7 +826,7 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
     st.block = shape.block;
     st.tile = shape.tile;
     const int64_t hb = std::min(ve, H) > vb ? (std::min(ve, H) - vb + R - 1) / R : 0;
-    st.launches = (std::max(vb, H) < ve ? 1 : 0) + 2 * hb;
+    st.launches = (std::max(vb, H) < ve ? 1 : 0) + 3 * hb;  // + one scan per batch
     st.scratch_bytes = (int64_t)need;
     st.total_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

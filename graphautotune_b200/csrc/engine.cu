@@ -28,6 +28,8 @@
 //
 // The kernel has no waits on other CTAs: the only inter-CTA interaction is
 // atomicAdd on the cursor and the totals.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <climits>
 #include <cstdio>
@@ -951,17 +953,36 @@ struct LineMarks {
     }
 };
 
-// Pass 1 over heavy roots [r0, r1): the units are the pairs (v0, v1 > v0),
+constexpr int kC4Piece = 1024;  // entries of a long list per pass-1b piece
+
+// Root of unit tu among [r0, r1): the largest v with up(v) <= tu.
+__device__ __forceinline__ int64_t c4_root_of(const int64_t *off, const int64_t *lo_off,
+                                              int64_t r0, int64_t r1, int64_t tu) {
+    int64_t lo = r0, n = r1 - r0;
+    while (n > 0) {
+        const int64_t h = n >> 1;
+        const int64_t m = lo + h;
+        const bool right = off[m + 1] - lo_off[m + 1] <= tu;
+        lo = right ? m + 1 : lo;
+        n = right ? n - h - 1 : h;
+    }
+    return min(lo, r1 - 1);
+}
+
+// Pass 1a over heavy roots [r0, r1): the units are the pairs (v0, v1 > v0),
 // numbered by up(v) = off[v] - lo_off[v] (upper neighbours before v).  A warp
-// takes `chunk` consecutive units; each lane resolves its own, walks short
-// neighbour lists alone and hands long ones (>= 64 entries above v0) to the
-// whole warp.
+// takes `chunk` consecutive units; each lane resolves its own and walks its
+// list above v0 alone when it is short (< 64 entries).  A long list (a hub
+// neighbour) is not walked here: the lane records how many kC4Piece-entry
+// pieces it has, and pass 1b spreads those pieces over the whole grid, so no
+// warp is left alone with a list of ~10^4 entries.
 template <bool STATS>
 __global__ void __launch_bounds__(256)
     c4_heavy_pass1_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
                           const int64_t *__restrict__ lo_off, int64_t r0, int64_t r1,
                           int64_t u_begin, int64_t u_end, int32_t chunk, DevCounters *ctr,
-                          uint32_t *rows, uint32_t *bms, int64_t stride, int64_t words) {
+                          uint32_t *rows, uint32_t *bms, int64_t stride, int64_t words,
+                          int32_t *npieces) {
     const int lane = threadIdx.x & 31;
     unsigned long long bytes = 0;
     LineMarks marks;
@@ -971,20 +992,7 @@ __global__ void __launch_bounds__(256)
         s = __shfl_sync(0xffffffffu, s, 0);
         if (s >= (unsigned long long)u_end) break;
         const int64_t e = min((int64_t)s + chunk, u_end);
-        // root of the first unit: largest v in [r0, r1) with up(v) <= s + lane
-        int64_t v0 = r0;
-        {
-            const int64_t tu = (int64_t)s + lane;
-            int64_t lo = r0, n = r1 - r0;
-            while (n > 0) {
-                const int64_t h = n >> 1;
-                const int64_t m = lo + h;
-                const bool right = off[m + 1] - lo_off[m + 1] <= tu;
-                lo = right ? m + 1 : lo;
-                n = right ? n - h - 1 : h;
-            }
-            v0 = min(lo, r1 - 1);
-        }
+        int64_t v0 = c4_root_of(off, lo_off, r0, r1, (int64_t)s + lane);
         for (int64_t base = (int64_t)s; base < e; base += 32) {
             const int64_t tu = base + lane;
             const bool live = tu < e;
@@ -1011,24 +1019,62 @@ __global__ void __launch_bounds__(256)
                 }
                 if (STATS) bytes += 12ull * (unsigned)(d1 - s1);
             }
-            unsigned big = __ballot_sync(0xffffffffu, longl);
-            while (big) {
-                const int src = __ffs(big) - 1;
-                big &= big - 1;
-                const int32_t bs = __shfl_sync(0xffffffffu, s1, src);
-                const int32_t bd = __shfl_sync(0xffffffffu, d1, src);
-                const int32_t br = __shfl_sync(0xffffffffu, row, src);
-                const int64_t bo = __shfl_sync(0xffffffffu, o1, src);
-                uint32_t *rw = rows + (int64_t)br * stride;
-                uint32_t *bm = bms + (int64_t)br * words;
-                for (int k = bs + lane; k < bd; k += 32) {
-                    const int32_t x = adj[bo + k];
-                    atomicAdd(&rw[x], 1u);
-                    marks.mark(bm, x);
-                }
-                if (STATS && lane == 0) bytes += 12ull * (unsigned)(bd - bs);
-            }
+            // long lists become pieces for pass 1b
+            if (live) npieces[tu - u_begin] = longl ? (d1 - s1 + kC4Piece - 1) / kC4Piece : 0;
         }
+    }
+    if (marks.bm) marks.flush();
+    if (STATS) {
+        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+        if (lane == 0) atomicAdd(&ctr->bytes, bytes);
+    }
+}
+
+// Pass 1b: the pieces of the long lists, pref[u] = pieces of units before u
+// (u counted from u_begin; pref[n_units] = all pieces).  A warp takes one
+// piece from the cursor, re-derives its unit (root, neighbour, start of the
+// list above the root) and adds its up to kC4Piece wedges.
+template <bool STATS>
+__global__ void __launch_bounds__(256)
+    c4_heavy_pass1b_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
+                           const int64_t *__restrict__ lo_off, int64_t r0, int64_t r1,
+                           int64_t u_begin, const int64_t *__restrict__ pref, int64_t n_units,
+                           DevCounters *ctr, uint32_t *rows, uint32_t *bms, int64_t stride,
+                           int64_t words) {
+    const int lane = threadIdx.x & 31;
+    const int64_t total = pref[n_units];
+    unsigned long long bytes = 0;
+    LineMarks marks;
+    for (;;) {
+        unsigned long long q = 0;
+        if (lane == 0) q = atomicAdd(&ctr->cursor, 1ull);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if ((int64_t)q >= total) break;
+        int64_t lo = 0, n = n_units;  // unit: last u with pref[u] <= q
+        while (n > 0) {
+            const int64_t h = n >> 1;
+            const bool right = pref[lo + h + 1] <= (int64_t)q;
+            lo = right ? lo + h + 1 : lo;
+            n = right ? n - h - 1 : h;
+        }
+        const int64_t tu = u_begin + lo;
+        const int64_t v0 = c4_root_of(off, lo_off, r0, r1, tu);
+        const int64_t j = tu - (off[v0] - lo_off[v0]);
+        const int32_t lo0 = (int32_t)(lo_off[v0 + 1] - lo_off[v0]);
+        const int32_t v1 = adj[off[v0] + lo0 + j];
+        const int64_t o1 = off[v1];
+        const int32_t d1 = (int32_t)(off[v1 + 1] - o1);
+        const int32_t s1 = upper_serial(adj + o1, d1, (int32_t)v0);
+        const int32_t b = s1 + (int32_t)((int64_t)q - pref[lo]) * kC4Piece;
+        const int32_t e = min(d1, b + kC4Piece);
+        uint32_t *rw = rows + (v0 - r0) * stride;
+        uint32_t *bm = bms + (v0 - r0) * words;
+        for (int k = b + lane; k < e; k += 32) {
+            const int32_t x = adj[o1 + k];
+            atomicAdd(&rw[x], 1u);
+            marks.mark(bm, x);
+        }
+        if (STATS && lane == 0) bytes += 12ull * (unsigned)(e - b);
     }
     if (marks.bm) marks.flush();
     if (STATS) {
@@ -1236,12 +1282,15 @@ int c4_occ(int block) {
 template <bool STATS>
 int c4_heavy_occ() {
     int a = 0, b = 0;
+    int c = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, c4_heavy_pass1_kernel<STATS>, 256,
                                                       0) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, c4_heavy_pass2_kernel<STATS>, 256,
+                                                      0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, c4_heavy_pass1b_kernel<STATS>, 256,
                                                       0) != cudaSuccess)
         return 0;
-    return min(a, b);
+    return min(min(a, b), c);
 }
 }  // namespace
 
@@ -1261,6 +1310,14 @@ int c4_blocks_per_sm(int tile, int block, bool stats) {
 
 int c4_heavy_blocks_per_sm(bool stats) {
     return stats ? c4_heavy_occ<true>() : c4_heavy_occ<false>();
+}
+
+size_t c4_scan_temp_bytes(int64_t n) {
+    size_t b = 0;
+    if (cub::DeviceScan::ExclusiveSum(nullptr, b, (const int32_t *)nullptr, (int64_t *)nullptr,
+                                      (int)std::max<int64_t>(n, 1)) != cudaSuccess)
+        return 0;
+    return b;
 }
 
 cudaError_t launch_c4(const C4Launch &L, cudaStream_t st) {
@@ -1296,16 +1353,32 @@ cudaError_t launch_c4(const C4Launch &L, cudaStream_t st) {
     for (int64_t r0 = L.v_begin; r0 < he; r0 += L.rows_per_batch) {
         const int64_t r1 = std::min(r0 + L.rows_per_batch, he);
         const int32_t R = (int32_t)(r1 - r0);
-        if ((e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess)
+        const int64_t u0 = up(r0), n_units = up(r1) - u0;
+        if ((e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess ||
+            (e = cudaMemsetAsync(L.npieces + n_units, 0, sizeof(int32_t), st)) != cudaSuccess)
             return e;
         if (L.stats)
             c4_heavy_pass1_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
-                g.off, g.adj, g.lo_off, r0, r1, up(r0), up(r1), 128, ctr, L.heavy_rows,
-                L.heavy_bms, L.stride, L.words);
+                g.off, g.adj, g.lo_off, r0, r1, u0, u0 + n_units, 128, ctr, L.heavy_rows,
+                L.heavy_bms, L.stride, L.words, L.npieces);
         else
             c4_heavy_pass1_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
-                g.off, g.adj, g.lo_off, r0, r1, up(r0), up(r1), 128, ctr, L.heavy_rows,
-                L.heavy_bms, L.stride, L.words);
+                g.off, g.adj, g.lo_off, r0, r1, u0, u0 + n_units, 128, ctr, L.heavy_rows,
+                L.heavy_bms, L.stride, L.words, L.npieces);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        size_t tb = L.scan_temp_bytes;
+        if ((e = cub::DeviceScan::ExclusiveSum(L.scan_temp, tb, L.npieces, L.pieces_pref,
+                                               (int)(n_units + 1), st)) != cudaSuccess ||
+            (e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess)
+            return e;
+        if (L.stats)
+            c4_heavy_pass1b_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
+                g.off, g.adj, g.lo_off, r0, r1, u0, L.pieces_pref, n_units, ctr,
+                L.heavy_rows, L.heavy_bms, L.stride, L.words);
+        else
+            c4_heavy_pass1b_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
+                g.off, g.adj, g.lo_off, r0, r1, u0, L.pieces_pref, n_units, ctr,
+                L.heavy_rows, L.heavy_bms, L.stride, L.words);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if (L.stats)
             c4_heavy_pass2_kernel<true><<<L.heavy_grid, 256, 0, st>>>(

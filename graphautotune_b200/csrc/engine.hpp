@@ -84,10 +84,16 @@ struct C4Launch {
     uint32_t *heavy_rows = nullptr;
     uint32_t *heavy_bms = nullptr;
     int64_t rows_per_batch = 1, words = 0;
+    int32_t *npieces = nullptr;       // per unit of a batch (+1), long-list pieces
+    int64_t *pieces_pref = nullptr;   // their exclusive prefix (+1)
+    void *scan_temp = nullptr;
+    size_t scan_temp_bytes = 0;
     bool stats = false;
 };
 int c4_blocks_per_sm(int tile, int block, bool stats);
 int c4_heavy_blocks_per_sm(bool stats);
+// Temp storage of the piece scan over up to n units.
+size_t c4_scan_temp_bytes(int64_t n);
 cudaError_t launch_c4(const C4Launch &launch, cudaStream_t st);
 
 // Batched launches: host code fills an array of batch_job_bytes()-sized job

@@ -184,7 +184,8 @@ def training_graphs(count: int, seed0: int = 1000, max_log2: int = 16) -> list[d
 
 
 def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
-            log=None, max_seconds: float = 0.0) -> tuple[np.ndarray, np.ndarray]:
+            log=None, max_seconds: float = 0.0, max_log2: int = 16
+            ) -> tuple[np.ndarray, np.ndarray]:
     """Times `runs` random (graph, pattern, configuration) counts (fewer if
     `max_seconds` > 0 runs out first)."""
     from graphautotune_b200.experiments import make_graph
@@ -192,7 +193,7 @@ def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
     rng = random.Random(seed)
     pats = g.enumerate_patterns(4) + g.enumerate_patterns(5)
     glist = []
-    for sp in training_graphs(graphs):
+    for sp in training_graphs(graphs, max_log2=max_log2):
         gr = make_graph(sp)
         gr.upload(degree_order=True)
         glist.append((gr, graph_features(gr)))
@@ -309,6 +310,8 @@ def main():
     c.add_argument("--out", default="costmodel_data.npz")
     c.add_argument("--seed", type=int, default=0)
     c.add_argument("--max-seconds", type=float, default=0.0)
+    c.add_argument("--max-log2", type=int, default=16)
+    c.add_argument("--max-ms", type=float, default=200.0)
     t = sub.add_parser("train")
     t.add_argument("data")
     t.add_argument("--out", default="costmodel.npz")
@@ -323,7 +326,7 @@ def main():
     torch.cuda.set_device(0)
     if a.cmd == "collect":
         X, T = collect(a.runs, a.seed, log=lambda s: print(s, file=sys.stderr, flush=True),
-                       max_seconds=a.max_seconds)
+                       max_seconds=a.max_seconds, max_log2=a.max_log2, max_ms=a.max_ms)
         np.savez(a.out, X=X, T=T)
         print(json.dumps({"runs": len(X), "features": X.shape[1], "out": a.out}))
     elif a.cmd == "train":

@@ -291,23 +291,34 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64):
     gr.upload(degree_order=True)
     gf = costmodel.graph_features(gr)
     emit(config="c5", graph="R-MAT scale 24, 12*2^24 samples (avg degree 24), seed 4", V=V,
-         E=E, max_degree=md, setup_s=time.time() - t0, slice=f"shard 0 of {parts}")
+         E=E, max_degree=md, setup_s=time.time() - t0)
     cands = c5_candidates()[:n_candidates]
+    default = tuner.default_point()
     for name, pat in C5_PATTERNS.items():
         s = g.Schedule(pat, "exact", stats_graph=gr)
         pf = costmodel.plan_features(s)
+        # The slice: the middle shard of P, P grown from `parts` until the
+        # default configuration counts it in under 3 s.
+        P = parts
+        while True:
+            sh = P // 2
+            t0 = time.time()
+            _, r = g.Executor(tuner.to_config(default)).count_shard(gr, s, sh, P)
+            if r.kernel_ms < 3000 or P >= parts << 8:
+                break
+            P <<= 2
 
         def measure(d):
             ex = g.Executor(tuner.to_config(d))
-            raw, r = ex.count_shard(gr, s, 0, parts)
-            raw2, r2 = ex.count_shard(gr, s, 0, parts)
+            raw, r = ex.count_shard(gr, s, sh, P)
+            raw2, r2 = ex.count_shard(gr, s, sh, P)
             assert raw == raw2
             return raw, min(r.kernel_ms, r2.kernel_ms)
 
-        default = tuner.default_point()
         raw0, t_default = measure(default)
+        emit(config="c5", pattern=name, slice=f"shard {sh} of {P}", default_ms=t_default)
         if t_default > 20000:
-            emit(config="c5", pattern=name, skipped="slice too slow", default_ms=t_default)
+            emit(config="c5", pattern=name, skipped="slice too slow")
             continue
         picked = costmodel.pick(model, gf, pf, cands)
         raw_p, t_pick = measure(picked)

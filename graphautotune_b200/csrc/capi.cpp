@@ -741,9 +741,12 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
     int64_t R = std::min<int64_t>(std::max<int64_t>(H, 1), (budget / 2) / heavy_row);
     if (light_grid < 1 || R < 1)
         return fail(GAT_ERR_MEMORY, "memory budget below the 4-cycle counters' minimum");
-    const int64_t light_bytes = light_grid * tiles_per_block * row_bytes;
-    const int64_t hrows_bytes = R * row_bytes;
-    const int64_t bms_bytes = ((R * words * 4 + 255) / 256) * 256;
+    // Every region starts on a 256-byte boundary (rows are V words, which for
+    // odd V would leave the 8-byte arrays after them misaligned).
+    auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+    const int64_t light_bytes = al(light_grid * tiles_per_block * row_bytes);
+    const int64_t hrows_bytes = al(R * row_bytes);
+    const int64_t bms_bytes = al(R * words * 4);
     // the largest number of (root, upper neighbour) units in one heavy batch
     int64_t max_units = 0;
     {
@@ -752,9 +755,9 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
         for (int64_t r0 = vb; r0 < he; r0 += R)
             max_units = std::max(max_units, up(std::min(r0 + R, he)) - up(r0));
     }
-    const int64_t np_bytes = (((max_units + 1) * 4 + 255) / 256) * 256;
-    const int64_t pref_bytes = (((max_units + 1) * 8 + 255) / 256) * 256;
-    const int64_t temp_bytes = (((int64_t)c4_scan_temp_bytes(max_units + 1) + 255) / 256) * 256;
+    const int64_t np_bytes = al((max_units + 1) * 4);
+    const int64_t pref_bytes = al((max_units + 1) * 8);
+    const int64_t temp_bytes = al((int64_t)c4_scan_temp_bytes(max_units + 1));
     const size_t need = size_t(light_bytes + hrows_bytes + bms_bytes + np_bytes + pref_bytes +
                                temp_bytes);
     cudaError_t ce;
@@ -806,6 +809,14 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
         return cuda_fail(ce, "4-cycle launch");
     }
     cudaEventRecord(e->ev1, strm);
+    // Counter rows and bitmaps are zero again; clear the piece arrays and the
+    // scan's temp storage too, so the whole scratch stays zero for the next
+    // count, whose layout may differ.
+    if ((ce = cudaMemsetAsync(tail, 0, size_t(np_bytes + pref_bytes + temp_bytes), strm)) !=
+        cudaSuccess) {
+        e->scratch_clean = false;
+        return cuda_fail(ce, "4-cycle scratch clear");
+    }
     if ((ce = cudaMemcpyAsync(e->host_ctr, e->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
                               strm)) != cudaSuccess ||
         (ce = cudaStreamSynchronize(strm)) != cudaSuccess) {

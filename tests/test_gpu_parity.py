@@ -261,7 +261,14 @@ def test_four_cycle_heavy_batches_and_row_scans(gat):
     plan = _executor(gat, special_kernels=0)
     cases = [(gat.Graph.erdos_renyi(600, 300.0, 11), 1 << 20),
              (gat.Graph.barabasi_albert(20000, 8, 12), 16 << 20),
-             (gat.Graph.rmat(14, 1 << 17, 0.57, 0.19, 0.19, 13), 0)]
+             (gat.Graph.rmat(14, 1 << 17, 0.57, 0.19, 0.19, 13), 0),
+             (gat.Graph.barabasi_albert(3001, 8, 21), 256 << 20)]  # odd V: unaligned rows
+    wants = [plan.count(g, s).count for g, _ in cases]
+    # one executor across graphs whose scratch layouts differ, twice over
+    shared = _executor(gat, memory_budget=256 << 20)
+    for _ in range(2):
+        for (g, _), want in zip(cases, wants):
+            assert shared.count(g, s).count == want
     for gi, (g, budget) in enumerate(cases):
         want = plan.count(g, s).count
         for tile, block in ((32, 256), (8, 128), (1, 64)):

@@ -1,0 +1,139 @@
+"""Host logic of the autotuner and the cost model, without a GPU: the config
+space and its md5 fingerprints, the record.json history, simulated-annealing
+proposals over a synthetic cost surface, the batch tuning loop with a fake
+measurement, feature vectors, and the batch model's aggregation."""
+import json
+import math
+import random
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def tuner(gat):
+    from graphautotune_b200 import tuner
+    return tuner
+
+
+def test_points_round_trip_through_config(tuner):
+    rng = random.Random(1)
+    assert tuner.valid(tuner.default_point())
+    for _ in range(200):
+        d = tuner.random_point(rng)
+        assert tuner.valid(d)
+        assert tuner.from_config(tuner.to_config(d)) == d
+        e = tuner.random_walk(d, rng)
+        assert tuner.valid(e)
+        assert sum(d[k] != e[k] for k in tuner.KEYS) == 1
+
+
+def test_fingerprint_is_md5_of_sorted_key_indices(tuner):
+    import hashlib
+
+    d = tuner.default_point()
+    idx = [tuner.SPACE[k].index(d[k]) for k in sorted(tuner.SPACE)]
+    want = hashlib.md5(",".join(map(str, idx)).encode()).hexdigest()
+    assert tuner.fingerprint(d) == want
+    rng = random.Random(2)
+    pts = {tuner.fingerprint(tuner.random_point(rng)) for _ in range(300)}
+    assert len(pts) > 100  # distinct points, distinct fingerprints
+
+
+def test_history_persists_as_record_json(tuner, tmp_path):
+    path = tmp_path / "run" / "record.json"
+    h = tuner.History(str(path))
+    rng = random.Random(3)
+    pts = [tuner.random_point(rng) for _ in range(5)]
+    for i, p in enumerate(pts):
+        h.add(p, 1.0 + i)
+    rec = json.loads(path.read_text())
+    assert [r[1] for r in rec] == [1.0, 2.0, 3.0, 4.0, 5.0]
+    h2 = tuner.History(str(path))
+    assert h2.best() == (pts[0], 1.0)
+    assert all(h2.seen(p) for p in pts)
+
+
+def _bowl(tuner):
+    """Synthetic cost: squared index distance to a fixed optimum."""
+    opt = {k: tuner.SPACE[k][len(tuner.SPACE[k]) // 2] for k in tuner.KEYS}
+    oi = tuner.index_list(opt)
+
+    def cost(d):
+        return float(sum((a - b) ** 2 for a, b in zip(tuner.index_list(d), oi)))
+    return opt, cost
+
+
+def test_annealing_proposals_descend_a_cost_surface(tuner):
+    opt, cost = _bowl(tuner)
+
+    class Model:
+        def predict(self, xs):
+            return [cost(x) for x in xs]
+
+    rng = random.Random(4)
+    h = tuner.History()
+    props = tuner.propose(Model(), h, 3, rng, n_iter=60)
+    assert len(props) == 3 and all(tuner.valid(p) for p in props)
+    base = np.mean([cost(tuner.random_point(random.Random(i))) for i in range(50)])
+    assert max(cost(p) for p in props) < base
+    # proposals are never points already measured
+    for p in props:
+        h.add(p, cost(p))
+    again = tuner.propose(Model(), h, 3, rng, n_iter=60)
+    assert not any(h.seen(p) for p in again)
+
+
+def test_tune_batch_loop_with_a_fake_measurement(tuner, monkeypatch):
+    opt, cost = _bowl(tuner)
+    calls = []
+
+    def fake_measure(b, d, reps=2):
+        calls.append(d)
+        return 1.0 + cost(d)
+
+    monkeypatch.setattr(tuner, "measure_batch", fake_measure)
+    cfg, hist = tuner.tune_batch(object(), budget=10, seed=5)
+    assert len(calls) == 10 and len(hist) == 10
+    assert tuner.fingerprint(calls[0]) == tuner.fingerprint(tuner.default_point())
+    best = min(calls, key=cost)
+    assert tuner.from_config(cfg) == best
+    assert len({tuner.fingerprint(c) for c in calls}) == 10  # no repeats
+
+
+def test_feature_vectors(gat):
+    from graphautotune_b200 import costmodel, tuner
+
+    g = gat.Graph.barabasi_albert(500, 4, 6)
+    gf = costmodel.graph_features(g)
+    assert gf.shape == (20,) and np.all(np.isfinite(gf))
+    for p in ("0111101111011110", "0100110110010110110010100"):
+        pf = costmodel.plan_features(gat.Schedule(p, "exact"))
+        assert pf.shape == (10,) and np.all(np.isfinite(pf))
+        x = costmodel.features(gf, pf, tuner.default_point())
+        assert x.shape == (costmodel.N_FEATURES,) and np.all(np.isfinite(x))
+    pts = costmodel.all_points()
+    assert len(pts) > 100 and all(tuner.valid(p) for p in pts)
+
+
+def test_batch_model_sums_predicted_job_times(gat):
+    from graphautotune_b200 import costmodel, tuner
+
+    class Fixed:
+        """Predicts log-time = first configuration feature + job offset."""
+
+        def predict(self, X):
+            return X[:, 0] + X[:, -1]
+
+    g1 = gat.Graph.barabasi_albert(300, 3, 7)
+    g2 = gat.Graph.rmat(9, 2048, 0.57, 0.19, 0.19, 8)
+    pf = costmodel.plan_features(gat.Schedule("0111101111011110", "exact"))
+    jobs = [(costmodel.graph_features(g1), pf), (costmodel.graph_features(g2), pf)]
+    bm = costmodel.BatchTunerModel(Fixed(), jobs)
+    rng = random.Random(9)
+    xs = [tuner.random_point(rng) for _ in range(4)]
+    got = bm.predict(xs)
+    for d, v in zip(xs, got):
+        per = [float(Fixed().predict(costmodel.features(gf, p, d)[None, :])[0])
+               for gf, p in jobs]
+        assert math.isclose(v, math.log(sum(math.exp(t) for t in per)), rel_tol=1e-9)

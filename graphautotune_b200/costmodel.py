@@ -6,7 +6,8 @@ data graph) to log run time.  It is trained on timings the engine itself
 records (`collect`), and used to rank candidate configurations (`pick`),
 replacing the reference tuner's XGBoost model over configuration indices
 (tuning/tuning/role/modeling.py:81-102); the measured-search tuner
-(graphautotune_b200.tuner) is its fallback and the judge of its ranking.
+(graphautotune_b200.tuner) is its fallback, and measured times are what its
+ranking is checked against.
 
     python -m graphautotune_b200.costmodel collect --runs 20000 --out data.npz
     python -m graphautotune_b200.costmodel train data.npz --out model.npz

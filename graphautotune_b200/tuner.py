@@ -1,12 +1,12 @@
 """In-process autotuner for launch shapes.
 
 Mirrors the reference tuner (tuning/tuning/): a discrete config space over
-flat dotted keys (tuning/tuning/config/base.py:221-262), the same md5
-fingerprint of the sorted-key index list (base.py:310-314), random warm-up
+flat dotted keys (tuning/tuning/config/base.py:170-222), the same md5
+fingerprint of the sorted-key index list (base.py:259-262), random warm-up
 configurations, simulated-annealing proposals ranked by a cost model
-(role/manipulator.py:195-263: temperature 0.1, x0.9 per step), and a
+(role/manipulator.py:63-131: temperature 0.1, x0.9 per step), and a
 record.json history of [value dict, seconds] pairs that is reloaded on start
-(role/modeling.py:342-373).  The differences: a configuration is applied at
+(role/modeling.py:48-79).  The differences: a configuration is applied at
 run time (no header export, no CMake rebuild per configuration), it is
 measured in process with CUDA events, and the cost model is pluggable
 (`model=`): by default the measured history itself (nearest measured point),

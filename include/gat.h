@@ -147,7 +147,7 @@ void gat_config_default(gat_config *c);
 /* This engine's tuned starting point (persistent grid, 32-lane tiles). */
 void gat_config_engine_default(gat_config *c);
 /* Parses either the designated-initializer text the tuner writes into
- * default_config.hpp (tuning/tuning/config/base.py:286-293, e.g.
+ * default_config.hpp (tuning/tuning/config/base.py:224-242, e.g.
  * "{.vertex_set_config = {.set_search_type = 64, ...}, ...}") or the flat
  * JSON value dict of config.json (tuning/tuning/role/driver.py:50-51, keys
  * like "engine_config.launch_config.num_blocks").  Unmentioned fields keep

@@ -2,7 +2,7 @@
 //
 //   pm <graph.bin> <pattern_adj> [hash_code] [--mode exact|ref]
 //      [--config <file with designated initializer or config.json>]
-//      [--results-dir DIR] [--text]
+//      [--results-dir DIR] [--text] [--variant N]
 //
 // Prints "Answer: N" and "Time: X us (Y s)" like the reference (pm.cu:70-82);
 // with a hash code it writes <results-dir>/<hash>/time.txt (seconds) and
@@ -11,7 +11,9 @@
 // call with the graph already resident, as in pm.cu:60-64.  The default mode
 // is ref (the reference's semantics); --mode exact gives subgraph counts.
 // Exit status is non-zero on any error, which the driver maps to an
-// infinite time (driver.py:118-122).
+// infinite time (driver.py:118-122).  --variant N (exact mode) counts with
+// exact plan variant N (gat_schedule_build_variant), so a process-based
+// tuner can time the variants too.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -44,6 +46,7 @@ static bool mkdir_p(const std::string &path) {
 int main(int argc, char **argv) {
     std::string graph, pattern, hash, results_dir = "tuning_results", config_file;
     int mode = GAT_MODE_REF_COMPAT;
+    int variant = 0;
     bool binary = true;
     int pos = 0;
     for (int i = 1; i < argc; i++) {
@@ -57,6 +60,8 @@ int main(int argc, char **argv) {
             results_dir = argv[++i];
         } else if (a == "--text") {
             binary = false;
+        } else if (a == "--variant" && i + 1 < argc) {
+            variant = std::atoi(argv[++i]);
         } else if (pos == 0) {
             graph = a;
             pos++;
@@ -71,7 +76,7 @@ int main(int argc, char **argv) {
     if (pos < 2) {
         std::fprintf(stderr, "Usage: pm <graph_name> <pattern_str> [hash_code] "
                              "[--mode exact|ref] [--config FILE] "
-                             "[--results-dir DIR] [--text]\n");
+                             "[--results-dir DIR] [--text] [--variant N]\n");
         return 2;
     }
     std::printf("Graph Name: %s\n", graph.c_str());
@@ -95,7 +100,7 @@ int main(int argc, char **argv) {
     gat_executor *e = nullptr;
     if (gat_pattern_from_adj(pattern.c_str(), &p) != GAT_OK) return die("pattern");
     if (gat_graph_load(graph.c_str(), binary ? 1 : 0, &g) != GAT_OK) return die("graph");
-    if (gat_schedule_build(p, mode, g, &s) != GAT_OK) return die("schedule");
+    if (gat_schedule_build_variant(p, mode, g, variant, &s) != GAT_OK) return die("schedule");
     int32_t V = 0, md = 0;
     int64_t E = 0;
     gat_graph_info(g, &V, &E, &md);

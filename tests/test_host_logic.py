@@ -196,3 +196,19 @@ def test_every_schedule_variant_is_exact(gat, oracle, golden_graphs):
             with pytest.raises(gat.GatError):
                 gat.Schedule(p, "exact", variant=n)
     assert checked > 20
+
+
+def test_pm_cli_rejects_unknown_schedule_variant():
+    """The pm-compatible CLI builds the schedule before touching the GPU; an
+    exact plan variant that does not exist fails with a non-zero exit (which
+    the reference's driver reads as an infinite time)."""
+    import subprocess
+
+    pm = ROOT / "graphautotune_b200" / "bin" / "pm"
+    graph = ROOT / "tests" / "golden" / "graphs" / "er60.bin"
+    r = subprocess.run([str(pm), str(graph), "0100110110010110110010100", "--mode", "exact",
+                        "--variant", "99"], capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0
+    assert "schedule variant out of range" in r.stderr
+    r = subprocess.run([str(pm)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "--variant" in r.stderr

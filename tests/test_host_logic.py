@@ -212,3 +212,19 @@ def test_pm_cli_rejects_unknown_schedule_variant():
     assert "schedule variant out of range" in r.stderr
     r = subprocess.run([str(pm)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 2 and "--variant" in r.stderr
+
+
+def test_config5_patterns_exact_on_cpu_model(gat, oracle, golden_graphs):
+    """The learned-cost-model workload's patterns (6-clique, 6-cycle with a
+    chord, 7-vertex triangle + path): the first exact plan variants,
+    interpreted on the CPU, give the oracle's count."""
+    from graphautotune_b200.experiments import C5_PATTERNS
+
+    for name in ("er60",):
+        off, adj = golden_graphs[name].csr()
+        for pname, p in C5_PATTERNS.items():
+            want = oracle.exact_count(off, adj, p)
+            for v in range(min(4, gat.Schedule.variants(p))):
+                raw, div = plan_model.run(
+                    plan_model.parse(gat.Schedule(p, "exact", variant=v).plan_bytes()), off, adj)
+                assert raw % div == 0 and raw // div == want, (name, pname, v)

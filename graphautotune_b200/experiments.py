@@ -208,9 +208,10 @@ def run_c4(args):
         # Launch shapes are timed on a sample batch: one slice of 1/P of every
         # job's work queue, slices spread over the queues.
         P = args.tune_parts
-        sample = g.Batch()
+        sample, screen = g.Batch(), g.Batch()
         for j, (gr, p) in enumerate((gr, p) for gr in graphs for p in pats):
             sample.add_shard(gr, tscheds[p], (j * 7) % P, P)
+            screen.add_shard(gr, tscheds[p], (j * 7) % (8 * P), 8 * P)
         model = None
         if args.model:
             # proposals ranked by the learned cost model (summed over the jobs)
@@ -221,7 +222,7 @@ def run_c4(args):
             model = costmodel.BatchTunerModel(costmodel.CostModel.load(args.model),
                                               [(gf, pfs[p]) for gf in gfs for p in pats])
         t = time.perf_counter()
-        cfg, hist = tuner.tune_batch(sample, budget=args.tune, model=model)
+        cfg, hist = tuner.tune_batch(sample, budget=args.tune, model=model, screen=screen)
         emit(config="c4", arm="tuner", sample=f"1/{P} of every job", history=hist,
              ranking="cost model" if model else "nearest measured point",
              tuning_s=time.perf_counter() - t)

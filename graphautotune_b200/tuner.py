@@ -196,12 +196,21 @@ def measure_batch(b: "g.Batch", d: dict, reps: int = 2) -> float:
 
 
 def tune_batch(b: "g.Batch", budget: int = 12, seed: int = 0, record: str | None = None,
-               model=None) -> tuple["g.Config", list]:
+               model=None, screen: "g.Batch | None" = None, screen_factor: float = 3.0
+               ) -> tuple["g.Config", list]:
     """Measures the default point, a few random warm-up points, then model-ranked
-    proposals, `budget` measurements in all; returns the best config."""
+    proposals, `budget` points in all; returns the best config.
+
+    With a `screen` batch (a much smaller sample of the same jobs), every
+    point is first timed there; a point more than `screen_factor` times
+    slower than the best screened point so far is not measured on `b` and
+    is recorded at its screened time scaled by the last measured
+    full-to-screen ratio (a bad launch shape can be 1000x slower than a good
+    one, and would otherwise dominate the tuning time)."""
     rng = random.Random(seed)
     hist = History(record)
     todo = [default_point()] + [random_point(rng) for _ in range(max(1, budget // 3))]
+    best_screen, ratio = math.inf, None
     while len(hist.xs) < budget:
         if not todo:
             m = model or NearestModel(hist)
@@ -211,7 +220,17 @@ def tune_batch(b: "g.Batch", budget: int = 12, seed: int = 0, record: str | None
         d = todo.pop(0)
         if hist.seen(d) or not valid(d):
             continue
-        hist.add(d, measure_batch(b, d))
+        ts = None
+        if screen is not None:
+            ts = measure_batch(screen, d, reps=1)
+            if ratio is not None and ts > screen_factor * best_screen:
+                hist.add(d, ts * ratio)
+                continue
+            best_screen = min(best_screen, ts)
+        y = measure_batch(b, d)
+        if ts:
+            ratio = y / ts
+        hist.add(d, y)
     best, _ = hist.best()
     return to_config(best), [[fingerprint(x), y] for x, y in zip(hist.xs, hist.ys)]
 

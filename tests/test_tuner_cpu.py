@@ -137,3 +137,29 @@ def test_batch_model_sums_predicted_job_times(gat):
         per = [float(Fixed().predict(costmodel.features(gf, p, d)[None, :])[0])
                for gf, p in jobs]
         assert math.isclose(v, math.log(sum(math.exp(t) for t in per)), rel_tol=1e-9)
+
+
+def test_tune_batch_screens_out_slow_points(tuner, monkeypatch):
+    """With a screen batch, points far slower than the best screened one are
+    never measured on the full sample."""
+    opt, cost = _bowl(tuner)
+    full, screen = object(), object()
+    full_calls = []
+
+    def fake_measure(b, d, reps=2):
+        t = 2.0 ** cost(d)  # steep: most random points are >3x the best
+        if b is full:
+            full_calls.append(d)
+            return 8.0 * t
+        return t
+
+    monkeypatch.setattr(tuner, "measure_batch", fake_measure)
+    cfg, hist = tuner.tune_batch(full, budget=12, seed=6, screen=screen)
+    assert len(hist) == 12
+    assert len(full_calls) < 12  # some points were screened out
+    best_full = min(full_calls, key=cost)
+    assert tuner.from_config(cfg) == best_full
+    # screened points carry an estimate on the full-sample scale
+    ys = dict(hist)
+    for d in full_calls:
+        assert math.isclose(ys[tuner.fingerprint(d)], 8.0 * 2.0 ** cost(d))

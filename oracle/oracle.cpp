@@ -409,7 +409,8 @@ int oracle_ref_engine(int32_t V, const int64_t *offs, const int32_t *adj,
 #pragma omp parallel num_threads(threads) reduction(+ : total, bytes)
     {
         RefUnit u(g, sd);
-#pragma omp for schedule(dynamic, 16)
+        // one root at a time: hub roots can hold most of the work
+#pragma omp for schedule(dynamic, 1)
         for (int32_t v0 = root_begin; v0 < root_end; v0++) {
             // first_extend_kernel (engine_kernel.cuh:40-60): prefix 0 is
             // N(v0), the level-0 embedding is v0.

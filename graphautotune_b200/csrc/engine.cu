@@ -210,10 +210,13 @@ __device__ __forceinline__ int isect_count(const Tile<G> &t, const int32_t *a,
     return t.sum(c);
 }
 
+// Stored outputs keep at most `cap` elements (the scratch slot's size); the
+// returned length is the full intersection size, so a caller sees an
+// overflow as a length above cap.
 template <int G>
 __device__ __forceinline__ int isect_store(const Tile<G> &t, const int32_t *a,
                                            int na, const int32_t *b, int nb,
-                                           int32_t *out, int linear_below) {
+                                           int32_t *out, int linear_below, int cap) {
     if (na > nb) {
         const int32_t *tp = a;
         a = b;
@@ -232,7 +235,8 @@ __device__ __forceinline__ int isect_store(const Tile<G> &t, const int32_t *a,
             f = contains(b, nb, x, linear_below);
         }
         const unsigned m = t.ballot(f);
-        if (f) out[n + __popc(m & ((1u << t.lane) - 1u))] = x;
+        const int at = n + __popc(m & ((1u << t.lane) - 1u));
+        if (f && at < cap) out[at] = x;
         n += __popc(m);
     }
     return n;
@@ -267,7 +271,7 @@ __device__ __forceinline__ int bitmap_count(const Tile<G> &t, const int32_t *pro
 template <int G>
 __device__ __forceinline__ int bitmap_store(const Tile<G> &t, const int32_t *probe,
                                             int np, const uint32_t *row,
-                                            int32_t *out) {
+                                            int32_t *out, int cap) {
     int n = 0;
     for (int base = 0; base < np; base += G) {
         const int i = base + t.lane;
@@ -278,7 +282,8 @@ __device__ __forceinline__ int bitmap_store(const Tile<G> &t, const int32_t *pro
             f = bit_set(row, x);
         }
         const unsigned m = t.ballot(f);
-        if (f) out[n + __popc(m & ((1u << t.lane) - 1u))] = x;
+        const int at = n + __popc(m & ((1u << t.lane) - 1u));
+        if (f && at < cap) out[at] = x;
         n += __popc(m);
     }
     return n;
@@ -371,8 +376,16 @@ __device__ void level_sets(const Tile<G> &t, TileSmem &S, const GatPlan &P,
                 if (STATS && t.lane == 0) bytes += 4ull * (unsigned)(nl + fl);
                 if (kind == GAT_SET_STORE) {
                     int32_t *out = scratch + (int64_t)P.p_slot[p] * a.cap;
-                    len = row ? bitmap_store(t, probe, np, row, out)
-                              : isect_store(t, nb, nl, fp, fl, out, a.linear_below);
+                    len = row ? bitmap_store(t, probe, np, row, out, a.cap)
+                              : isect_store(t, nb, nl, fp, fl, out, a.linear_below, a.cap);
+                    if (len > a.cap) {
+                        // The slot is smaller than the set (a caller stated a
+                        // maximum degree below the graph's): the count is
+                        // void, and the set is cut so no access leaves it.
+                        if (t.lane == 0 && a.ctr != nullptr)
+                            atomicOr(&a.ctr->error, GAT_DEVERR_SCRATCH);
+                        len = a.cap;
+                    }
                     ptr = out;
                     if (STATS && t.lane == 0) bytes += 4ull * (unsigned)len;
                 } else {
@@ -1148,14 +1161,11 @@ template <int G, bool STATS>
 cudaError_t launch_one(const SearchArgs &a, int grid, int block,
                        cudaStream_t stream) {
     const size_t smem = size_t(block / G) * sizeof(TileSmem);
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(
-            search_kernel<G, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            227 * 1024);
-        if (e != cudaSuccess) return e;
-        attr_done = true;
-    }
+    // Set on every launch: the attribute belongs to the current device's
+    // context, and a process may count on several devices or reset one.
+    cudaError_t e = cudaFuncSetAttribute(
+        search_kernel<G, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
     search_kernel<G, STATS><<<grid, block, smem, stream>>>(a);
     return cudaGetLastError();
 }
@@ -1495,6 +1505,16 @@ static_assert(kNoAllocPlanOffset + sizeof(GatPlan) <= kNoAllocScratchOffset, "pl
 std::mutex g_noalloc_mu;
 unsigned char *g_noalloc_base[256] = {};  // per device ordinal
 
+// Writes the plan into the static array from the launch's own parameter
+// block, so no host buffer has to outlive the call.
+__global__ void noalloc_store_plan(const GatPlan plan, GatPlan *dst) {
+    constexpr int kWords = int(sizeof(GatPlan) / sizeof(uint32_t));
+    static_assert(sizeof(GatPlan) % sizeof(uint32_t) == 0, "plan is whole words");
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(&plan);
+    uint32_t *out = reinterpret_cast<uint32_t *>(dst);
+    for (int i = threadIdx.x; i < kWords; i += blockDim.x) out[i] = src[i];
+}
+
 __global__ void noalloc_finish(const DevCounters *c, long long divisor, long long *out) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         const long long raw = (long long)c->result;
@@ -1567,10 +1587,10 @@ int count_noalloc(const GatPlan &plan, const int64_t *d_off, const int32_t *d_ad
     if (e != cudaSuccess) return bad(GAT_ERR_CUDA, cudaGetErrorString(e));
     DevCounters *ctr = reinterpret_cast<DevCounters *>(base);
     GatPlan *dplan = reinterpret_cast<GatPlan *>(base + kNoAllocPlanOffset);
-    if ((e = cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(dplan, &plan, sizeof(GatPlan), cudaMemcpyHostToDevice,
-                             stream)) != cudaSuccess)
+    if ((e = cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream)) != cudaSuccess)
         return bad(GAT_ERR_CUDA, cudaGetErrorString(e));
+    noalloc_store_plan<<<1, 128, 0, stream>>>(plan, dplan);
+    if ((e = cudaGetLastError()) != cudaSuccess) return bad(GAT_ERR_CUDA, cudaGetErrorString(e));
     SearchArgs a{};
     a.plan = dplan;
     a.off = d_off;

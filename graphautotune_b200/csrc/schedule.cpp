@@ -240,56 +240,71 @@ std::vector<Pairs> restriction_candidates(const Pattern &p) {
 
 }  // namespace
 
+namespace {
+
+// Survival fractions of a restriction list: f[i] = the share of the n!
+// labellings of the pattern's vertices by 0..n-1 in which restrictions
+// 0..i all hold (value of .first above value of .second), then made
+// conditional: f[i] / f[i-1].  Counts are integers and n! is exact in a
+// double, so the shares are computed as count / n! before the division.
+std::vector<double> survival_fractions(int n, const Pairs &rs) {
+    const int nr = (int)rs.size();
+    std::vector<double> f(nr, 0.0);
+    std::vector<int> lab(n);
+    std::iota(lab.begin(), lab.end(), 0);
+    do {
+        int held = 0;
+        while (held < nr && lab[rs[held].first] > lab[rs[held].second]) held++;
+        for (int i = 0; i < held; i++) f[i] += 1;
+    } while (std::next_permutation(lab.begin(), lab.end()));
+    double orders = 1;
+    for (int i = 2; i <= n; i++) orders *= i;
+    for (double &x : f) x /= orders;
+    for (int i = nr - 1; i > 0; --i) f[i] /= f[i - 1];
+    return f;
+}
+
+// Position (1-based, counting upwards) of vertex j among the earlier
+// neighbours of vertex u, or 0 when j is not one of them.
+int backward_rank(const Pattern &p, int j, int u) {
+    if (j >= u || !p.has(j, u)) return 0;
+    int r = 0;
+    for (int x = 0; x <= j; x++) r += p.has(x, u) ? 1 : 0;
+    return r;
+}
+
+}  // namespace
+
+// The reference's cost formula for a vertex order with restrictions
+// (core/schedule.hpp:362-437), on a random graph with edge density
+// p0 = E / V^2 and triangle closure p1 = tri * V / E^2.  Levels are visited
+// from the last enumerated one down to level 0; each level adds the search
+// cost of every later enumerated vertex that intersects with it (visited in
+// decreasing order), is thinned by the survival fractions of the
+// restrictions on it, and is multiplied by its expected candidate count.
+// The operation order is the reference's: the ranking of candidate orders
+// compares these doubles, so any reordering could pick another schedule.
 double estimate_restrictions(const Pattern &p, const Pairs &restrictions,
                              int v_cnt, int64_t e_cnt, long long tri_cnt) {
-    const int size = p.n;
-    const int suffix = iep_suffix_count(p);
+    const int n = p.n;
+    const int enumerated = n - iep_suffix_count(p);
     Pairs rs = restrictions;
+    std::sort(rs.begin(), rs.end());
+    const std::vector<double> keep = survival_fractions(n, rs);
     const double p0 = e_cnt * 1.0 / v_cnt / v_cnt;
     const double p1 = tri_cnt * 1.0 * v_cnt / e_cnt / e_cnt;
-    const int nr = (int)rs.size();
-    std::sort(rs.begin(), rs.end());
-    // sum[i]: fraction of orders in which restrictions 0..i all hold with
-    // value[first] > value[second], then turned into conditional fractions.
-    std::vector<double> sum(nr, 0.0);
-    std::vector<int> t(size);
-    std::iota(t.begin(), t.end(), 0);
-    do {
-        for (int i = 0; i < nr; i++) {
-            if (t[rs[i].first] > t[rs[i].second])
-                sum[i] += 1;
-            else
-                break;
-        }
-    } while (std::next_permutation(t.begin(), t.end()));
-    double total = 1;
-    for (int i = 2; i <= size; i++) total *= i;
-    for (int i = 0; i < nr; i++) sum[i] = sum[i] / total;
-    for (int i = nr - 1; i > 0; --i) sum[i] /= sum[i - 1];
-
-    std::vector<std::vector<int>> inv(size);
     double val = 1;
-    for (int i = size - suffix - 1; i >= 0; --i) {
-        int fwd = 0;
-        for (int j = 0; j < i; j++)
-            if (p.has(j, i)) ++fwd;
-        int c = fwd;
-        for (int j = i - 1; j >= 0; --j)
-            if (p.has(j, i)) {
-                inv[j].push_back(c);
-                c--;
-            }
-        for (size_t j = 0; j < inv[i].size(); j++) {
-            if (inv[i][j] > 1)
-                val += v_cnt * p0 * std::pow(p1, inv[i][j] - 2) *
-                       std::log2(p0 * v_cnt);
+    for (int level = enumerated - 1; level >= 0; --level) {
+        for (int later = enumerated - 1; later > level; --later) {
+            const int r = backward_rank(p, level, later);
+            if (r > 1)
+                val += v_cnt * p0 * std::pow(p1, r - 2) * std::log2(p0 * v_cnt);
         }
-        for (int j = 0; j < nr; j++)
-            if (rs[j].second == i) val *= sum[j];
-        if (i)
-            val *= v_cnt * p0 * std::pow(p1, fwd - 1);
-        else
-            val *= v_cnt;
+        for (size_t j = 0; j < rs.size(); j++)
+            if (rs[j].second == level) val *= keep[j];
+        int fwd = 0;
+        for (int j = 0; j < level; j++) fwd += p.has(j, level) ? 1 : 0;
+        val *= level ? v_cnt * p0 * std::pow(p1, fwd - 1) : (double)v_cnt;
     }
     return val;
 }

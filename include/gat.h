@@ -322,13 +322,19 @@ const char *gat_mlp_last_error(void);
  * until every resident tile's stored sets (stored prefixes x max_degree
  * ints) fit in the array; a schedule whose single CTA would not fit is
  * rejected with GAT_ERR_MEMORY.  Hub bitmaps are not used.
+ * max_degree must be at least the graph's largest row length: it sizes each
+ * tile's slots.  The kernel never writes past a slot; when a set would
+ * exceed one (max_degree stated too small) it reports an internal error and
+ * *d_count receives INT64_MIN.
  * The first call on each device looks up the array's device address
  * (cudaGetSymbolAddress), so make that first call before any stream capture
  * on the device.  Every call reuses the same array, so calls whose work
  * overlaps on the GPU (other streams, other host threads) race and return
  * wrong counts: serialise them.  *d_count (device memory, written in order on
  * `stream`) receives the count gat_executor_count would return, or
- * INT64_MIN if the kernel reported an internal error.  Nothing in this call
+ * INT64_MIN if the kernel reported an internal error.  The plan travels in
+ * a kernel's parameter block, so the schedule may be freed once the call
+ * returns.  Nothing in this call
  * allocates (no cudaMalloc/cudaFree, no allocating library routine). */
 #define GAT_NOALLOC_SCRATCH_BYTES (64u << 20)
 int gat_count_noalloc(const int64_t *d_offsets, const int32_t *d_adj, int32_t V,

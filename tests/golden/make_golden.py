@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference itself.
 
-Needs the reference sources (default /root/reference, or $GAT_REFERENCE) to
-build oracle/_ref/ (oracle/Makefile target `ref`).  Writes:
+Needs the reference sources where oracle/Makefile finds them (its REF, or
+$GAT_REFERENCE) to build oracle/_ref/ (target `ref`).  Writes:
 
   graphs/*.bin            small seeded graphs in the reference binary layout
   ref_schedules.jsonl     the reference's Core::Schedule for every pattern in
@@ -31,7 +31,8 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
 
-REF = Path(os.environ.get("GAT_REFERENCE", "/root/reference"))
+REF = Path(subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "print-ref"],
+                          capture_output=True, text=True, check=True).stdout.strip())
 
 # Pattern strings named in the reference's scripts and in the benchmark
 # configurations (scripts/run_pattern_matching.sh:14-21).

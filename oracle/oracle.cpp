@@ -268,6 +268,107 @@ struct RefUnit {
     }
 };
 
+// -------------------------------------------------------- order-restricted
+// labelled counting (full-size pins of the exact plans)
+//
+// Labelled embeddings f of the pattern, vertex by vertex in pattern order,
+// with f(a) < f(b) for every listed pair.  Candidates for vertex k come from
+// the shortest neighbour list among its earlier pattern neighbours, cut to
+// the open interval the pairs already allow; the others are checked with
+// has_edge.  The last vertex is counted, not recursed into.  None of this
+// shares code or structure with the engine's prefix sets or its
+// inclusion-exclusion.
+struct Restricted {
+    const CSR &g;
+    const Pat &p;
+    int lower[10][10];  // lower[k] = earlier a with f(a) < f(k)
+    int nlower[10] = {};
+    int upper[10][10];  // upper[k] = earlier b with f(k) < f(b)
+    int nupper[10] = {};
+    int32_t f[10];
+    Restricted(const CSR &g_, const Pat &p_, const int32_t *less, int32_t nless)
+        : g(g_), p(p_) {
+        for (int i = 0; i < nless; i++) {
+            const int a = less[2 * i], b = less[2 * i + 1];
+            if (a < b)
+                lower[b][nlower[b]++] = a;
+            else
+                upper[a][nupper[a]++] = b;
+        }
+    }
+    uint64_t place(int k) {
+        int src = -1;
+        for (int j = 0; j < k; j++)
+            if (p.e[j][k] && (src < 0 || g.deg(f[j]) < g.deg(f[src]))) src = j;
+        int64_t lo = -1, hi = g.V;  // open interval (lo, hi)
+        for (int i = 0; i < nlower[k]; i++) lo = std::max<int64_t>(lo, f[lower[k][i]]);
+        for (int i = 0; i < nupper[k]; i++) hi = std::min<int64_t>(hi, f[upper[k][i]]);
+        if (hi - lo < 2) return 0;
+        const int32_t *b, *e;
+        std::vector<int32_t> all;
+        if (src >= 0) {
+            const int32_t *nb = g.nb(f[src]);
+            b = std::upper_bound(nb, nb + g.deg(f[src]), (int32_t)lo);
+            e = std::lower_bound(b, nb + g.deg(f[src]), (int32_t)hi);
+        } else {
+            all.resize(size_t(hi - lo - 1));
+            std::iota(all.begin(), all.end(), (int32_t)(lo + 1));
+            b = all.data();
+            e = b + all.size();
+        }
+        uint64_t n = 0;
+        for (const int32_t *it = b; it < e; ++it) {
+            const int32_t x = *it;
+            bool ok = true;
+            for (int j = 0; j < k && ok; j++)
+                ok = f[j] != x && (!p.e[j][k] || j == src || g.has_edge(f[j], x));
+            if (!ok) continue;
+            if (k + 1 == p.n) {
+                n++;
+            } else {
+                f[k] = x;
+                n += place(k + 1);
+            }
+        }
+        return n;
+    }
+};
+
+// Sum over roots v0 in [rb, re) of sum_x C(c(v0, x), 2), where c counts the
+// common neighbours v1 of v0 and x with v1 and x both above v0 (at_largest
+// = 0) or both below it (at_largest = 1): every 4-cycle once, at its
+// smallest (largest) vertex and the vertex opposite it.
+uint64_t c4_rooted(const CSR &g, int32_t rb, int32_t re, bool at_largest, int threads) {
+    uint64_t total = 0;
+#pragma omp parallel num_threads(threads) reduction(+ : total)
+    {
+        std::vector<uint32_t> c(size_t(g.V), 0);
+        std::vector<int32_t> touched;
+#pragma omp for schedule(dynamic, 1)
+        for (int32_t v0 = rb; v0 < re; v0++) {
+            touched.clear();
+            const int32_t *n0 = g.nb(v0);
+            const int64_t d0 = g.deg(v0);
+            for (int64_t i = 0; i < d0; i++) {
+                const int32_t v1 = n0[i];
+                if (at_largest ? v1 >= v0 : v1 <= v0) continue;
+                const int32_t *n1 = g.nb(v1);
+                const int64_t d1 = g.deg(v1);
+                for (int64_t j = 0; j < d1; j++) {
+                    const int32_t x = n1[j];
+                    if (at_largest ? x >= v0 : x <= v0) continue;
+                    if (c[x]++ == 0) touched.push_back(x);
+                }
+            }
+            for (int32_t x : touched) {
+                total += uint64_t(c[x]) * (c[x] - 1) / 2;
+                c[x] = 0;
+            }
+        }
+    }
+    return total;
+}
+
 }  // namespace
 
 extern "C" {
@@ -432,6 +533,92 @@ int32_t oracle_intersect_size(const int32_t *a, int32_t na, const int32_t *b,
     for (int32_t i = 0; i < na; i++)
         if (std::binary_search(b, b + nb, a[i])) c++;
     return c;
+}
+
+uint64_t oracle_restricted_labelled(int32_t V, const int64_t *offs, const int32_t *adj,
+                                    const char *pattern, const int32_t *less,
+                                    int32_t nless, int32_t root_begin, int32_t root_end,
+                                    int threads) {
+    Pat p(pattern);
+    if (p.n < 2 || nless < 0) return 0;
+    for (int i = 0; i < 2 * nless; i++)
+        if (less[i] < 0 || less[i] >= p.n) return 0;
+    CSR g{V, offs, adj};
+    root_begin = std::max(root_begin, 0);
+    root_end = std::min(root_end, V);
+    if (root_begin >= root_end) return 0;
+    if (threads <= 0) threads = omp_get_max_threads();
+    // Work units: (root, index of the level-1 candidate in N(root)) when
+    // pattern vertex 1 is adjacent to vertex 0 (hub roots then spread over
+    // the threads), else one unit per root.
+    const bool by_edge = p.e[0][1];
+    std::vector<int64_t> start(size_t(root_end - root_begin) + 1, 0);
+    for (int32_t v = root_begin; v < root_end; v++)
+        start[v - root_begin + 1] = start[v - root_begin] + (by_edge ? g.deg(v) : 1);
+    const int64_t units = start.back();
+    uint64_t total = 0;
+#pragma omp parallel num_threads(threads) reduction(+ : total)
+    {
+        Restricted r(g, p, less, nless);
+        int32_t row = root_begin;
+#pragma omp for schedule(dynamic, 256)
+        for (int64_t u = 0; u < units; u++) {
+            if (start[row - root_begin] > u || start[row - root_begin + 1] <= u)
+                row = root_begin + int32_t(std::upper_bound(start.begin(), start.end(), u) -
+                                           start.begin() - 1);
+            r.f[0] = row;
+            if (!by_edge) {
+                total += r.place(1);
+                continue;
+            }
+            const int32_t x = g.nb(row)[u - start[row - root_begin]];
+            bool ok = x != row;
+            for (int i = 0; i < r.nlower[1] && ok; i++) ok = x > r.f[r.lower[1][i]];
+            for (int i = 0; i < r.nupper[1] && ok; i++) ok = x < r.f[r.upper[1][i]];
+            if (!ok) continue;
+            if (p.n == 2) {
+                total += 1;
+                continue;
+            }
+            r.f[1] = x;
+            total += r.place(2);
+        }
+    }
+    return total;
+}
+
+uint64_t oracle_c4_rooted(int32_t V, const int64_t *offs, const int32_t *adj,
+                          int32_t root_begin, int32_t root_end, int at_largest,
+                          int threads) {
+    CSR g{V, offs, adj};
+    root_begin = std::max(root_begin, 0);
+    root_end = std::min(root_end, V);
+    if (root_begin >= root_end) return 0;
+    if (threads <= 0) threads = omp_get_max_threads();
+    return c4_rooted(g, root_begin, root_end, at_largest != 0, threads);
+}
+
+int oracle_degree_order(int32_t V, const int64_t *offs, const int32_t *adj,
+                        int64_t *new_offs, int32_t *new_adj) {
+    if (V < 0) return -1;
+    std::vector<int32_t> by_rank(static_cast<size_t>(V));
+    std::iota(by_rank.begin(), by_rank.end(), 0);
+    std::stable_sort(by_rank.begin(), by_rank.end(), [&](int32_t a, int32_t b) {
+        return offs[a + 1] - offs[a] > offs[b + 1] - offs[b];
+    });
+    std::vector<int32_t> rank(static_cast<size_t>(V));
+    for (int32_t r = 0; r < V; r++) rank[by_rank[r]] = r;
+    new_offs[0] = 0;
+    for (int32_t r = 0; r < V; r++)
+        new_offs[r + 1] = new_offs[r] + (offs[by_rank[r] + 1] - offs[by_rank[r]]);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int32_t r = 0; r < V; r++) {
+        const int32_t v = by_rank[r];
+        int32_t *out = new_adj + new_offs[r];
+        for (int64_t i = offs[v]; i < offs[v + 1]; i++) *out++ = rank[adj[i]];
+        std::sort(new_adj + new_offs[r], new_adj + new_offs[r + 1]);
+    }
+    return 0;
 }
 
 }  // extern "C"

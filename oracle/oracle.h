@@ -76,6 +76,34 @@ int oracle_ref_engine(int32_t V, const int64_t *offs, const int32_t *adj,
                       int32_t root_end, int threads, int64_t *out,
                       uint64_t *balg);
 
+/* Labelled embeddings f of the pattern with f(0) in [root_begin, root_end)
+ * and f(less[2i]) < f(less[2i+1]) for every i < nless (pattern vertex
+ * indices).  With an exact plan's vertex order and symmetry-breaking
+ * conditions, this is the plan's undivided total over those roots; it is
+ * found by plain backtracking (candidates from neighbour lists, the last
+ * vertex counted), sharing nothing with the engine's prefix sets or
+ * inclusion-exclusion.  Summed over all roots and divided by the plan's
+ * divisor it is naive_pm's Answer / |Aut|. */
+uint64_t oracle_restricted_labelled(int32_t V, const int64_t *offs, const int32_t *adj,
+                                    const char *pattern, const int32_t *less,
+                                    int32_t nless, int32_t root_begin, int32_t root_end,
+                                    int threads);
+
+/* 4-cycles counted at a corner: for each v0 in [root_begin, root_end),
+ * sum over x of C(c, 2), c = common neighbours v1 of v0 and x with v1 and x
+ * above v0 (at_largest = 0: cycles whose smallest vertex is v0) or below it
+ * (at_largest = 1: cycles whose largest vertex is v0).  Over all roots both
+ * give the 4-cycle count (naive_pm's Answer / 8). */
+uint64_t oracle_c4_rooted(int32_t V, const int64_t *offs, const int32_t *adj,
+                          int32_t root_begin, int32_t root_end, int at_largest,
+                          int threads);
+
+/* The graph relabelled by decreasing degree, ties by smaller id first
+ * (vertex r of the result is the r-th in that order), rows sorted.  Writes
+ * V+1 offsets and E neighbours. */
+int oracle_degree_order(int32_t V, const int64_t *offs, const int32_t *adj,
+                        int64_t *new_offs, int32_t *new_adj);
+
 /* |a n b| for two sorted int32 lists (array_vertex_set.cuh:160-200). */
 int32_t oracle_intersect_size(const int32_t *a, int32_t na, const int32_t *b,
                               int32_t nb);

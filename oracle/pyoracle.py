@@ -41,6 +41,14 @@ def lib():
         l.oracle_ref_engine.restype = C.c_int
         l.oracle_ref_engine.argtypes = [C.c_int32, i64p, i32p, i32p, C.c_int32, C.c_int32,
                                         C.c_int32, C.c_int, i64p, C.POINTER(C.c_uint64)]
+        l.oracle_restricted_labelled.restype = C.c_uint64
+        l.oracle_restricted_labelled.argtypes = [C.c_int32, i64p, i32p, C.c_char_p, i32p,
+                                                 C.c_int32, C.c_int32, C.c_int32, C.c_int]
+        l.oracle_c4_rooted.restype = C.c_uint64
+        l.oracle_c4_rooted.argtypes = [C.c_int32, i64p, i32p, C.c_int32, C.c_int32, C.c_int,
+                                       C.c_int]
+        l.oracle_degree_order.restype = C.c_int
+        l.oracle_degree_order.argtypes = [C.c_int32, i64p, i32p, i64p, i32p]
         l.oracle_intersect_size.restype = C.c_int32
         l.oracle_intersect_size.argtypes = [i32p, C.c_int32, i32p, C.c_int32]
         _lib = l
@@ -122,3 +130,48 @@ def intersect_size(a, b) -> int:
     b = np.ascontiguousarray(b, np.int32)
     return lib().oracle_intersect_size(a.ctypes.data_as(C.POINTER(C.c_int32)), len(a),
                                        b.ctypes.data_as(C.POINTER(C.c_int32)), len(b))
+
+
+def restricted_labelled(off, adj, pattern: str, less, roots=None, threads: int = 0) -> int:
+    """Labelled embeddings f of `pattern` with f(0) in roots=(begin, end) and
+    f(a) < f(b) for every (a, b) in `less` (see oracle.h)."""
+    V, o, a, po, pa = _csr(off, adj)
+    b, e = roots if roots else (0, V)
+    flat = np.ascontiguousarray(np.array(less, np.int32).reshape(-1) if len(less)
+                                else np.zeros(2, np.int32))
+    return lib().oracle_restricted_labelled(V, po, pa, pattern.encode(),
+                                            flat.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            len(less), b, e, threads)
+
+
+def c4_rooted(off, adj, roots=None, at_largest: bool = False, threads: int = 0) -> int:
+    """4-cycles whose smallest (at_largest: largest) vertex lies in roots."""
+    V, o, a, po, pa = _csr(off, adj)
+    b, e = roots if roots else (0, V)
+    return lib().oracle_c4_rooted(V, po, pa, b, e, 1 if at_largest else 0, threads)
+
+
+def degree_order(off, adj):
+    """(offsets, neighbours) relabelled by decreasing degree, ties by id."""
+    V, o, a, po, pa = _csr(off, adj)
+    no = np.empty(V + 1, np.int64)
+    na = np.empty(max(int(o[-1]), 1), np.int32)
+    rc = lib().oracle_degree_order(V, po, pa, no.ctypes.data_as(C.POINTER(C.c_int64)),
+                                   na.ctypes.data_as(C.POINTER(C.c_int32)))
+    assert rc == 0
+    return no, na[:int(o[-1])]
+
+
+def plan_conditions(dump: dict) -> tuple[str, list[tuple[int, int]]]:
+    """For an exact schedule dump: the pattern in the plan's vertex order
+    (vertex i of the input becomes perm[i]) and its order conditions as
+    pairs (a, b) meaning f(a) < f(b).  The dump's restriction (i, u) means
+    the vertex at level u takes a smaller id than the one at level i."""
+    pat, perm = dump["pattern"], dump["perm"]
+    n = len(perm)
+    q = ["0"] * (n * n)
+    for i in range(n):
+        for j in range(n):
+            if pat[i * n + j] == "1" or pat[j * n + i] == "1":
+                q[perm[i] * n + perm[j]] = "1"
+    return "".join(q), [(u, i) for i, u in dump["restrictions"]]

@@ -15,8 +15,15 @@
 //                     [threads]
 //   samples v0 = first_v0 + i*stride, i in [0, num_v0), v0 < V
 //        naive_sample <graph.bin> <pattern_adj> - <threads>
-//   reads the roots (one per line) from stdin
-// prints one line: "labelled <sum> seconds <t> roots <k> threads <T>"
+//   reads work units from stdin, one per line: "v0" (a whole root) or
+//   "v0 v1" (the embeddings whose pattern vertices 0 and 1 map to v0 and v1:
+//   pattern_matching_func(2, {v0, v1}, ...), which is the part of root v0's
+//   search below the level-1 candidate v1; the caller passes only v1 that
+//   the matcher's level-1 checks accept), optionally followed by a group id
+//   in [0, 64) (default 0)
+// prints one line: "labelled <sum> seconds <t> roots <k> threads <T>", then
+// one line per group that had units: "group <g> labelled <sum> thread_seconds
+// <s> units <n>" (thread_seconds sums the per-unit wall times)
 #include <omp.h>
 
 #include <chrono>
@@ -24,6 +31,7 @@
 #include <cstdlib>
 #include <fstream>
 #include <iostream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -47,13 +55,24 @@ int main(int argc, char **argv) {
     }
     Infra::GlobalMemoryGraph<default_config> g{f, true};
     Core::Pattern p{std::string(argv[2])};
-    std::vector<long long> roots;
+    std::vector<long long> roots, second;  // second[i] < 0: whole root
+    std::vector<int> group;
     int threads = omp_get_max_threads();
     if (from_stdin) {
         if (argc > 4) threads = std::atoi(argv[4]);
-        long long v;
-        while (std::cin >> v)
-            if (v >= 0 && v < g.v_cnt()) roots.push_back(v);
+        std::string line;
+        while (std::getline(std::cin, line)) {
+            std::istringstream is(line);
+            long long v, w;
+            if (!(is >> v) || v < 0 || v >= g.v_cnt()) continue;
+            int grp = 0;
+            if (!(is >> w)) w = -1;
+            else if (!(is >> grp) || grp < 0 || grp >= 64) grp = 0;
+            if (w >= g.v_cnt()) continue;
+            roots.push_back(v);
+            second.push_back(w);
+            group.push_back(grp);
+        }
     } else {
         long long first = std::atoll(argv[3]);
         long long num = std::atoll(argv[4]);
@@ -63,19 +82,42 @@ int main(int argc, char **argv) {
             long long v = first + i * stride;
             if (v >= g.v_cnt()) break;
             roots.push_back(v);
+            second.push_back(-1);
+            group.push_back(0);
         }
     }
+    std::vector<long long> g_lab(64, 0), g_units(64, 0);
+    std::vector<double> g_sec(64, 0.0);
     long long total = 0;
     auto t0 = std::chrono::steady_clock::now();
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) \
     num_threads(threads)
     for (long long i = 0; i < (long long)roots.size(); i++) {
+        auto u0 = std::chrono::steady_clock::now();
         std::vector<int> choose{(int)roots[i]};
-        total += pattern_matching_func(1, choose, g, p);
+        long long c;
+        if (second[i] >= 0) {
+            choose.push_back((int)second[i]);
+            c = pattern_matching_func(2, choose, g, p);
+        } else {
+            c = pattern_matching_func(1, choose, g, p);
+        }
+        total += c;
+        double us = std::chrono::duration<double>(std::chrono::steady_clock::now() - u0).count();
+#pragma omp critical
+        {
+            g_lab[group[i]] += c;
+            g_sec[group[i]] += us;
+            g_units[group[i]]++;
+        }
     }
     auto t1 = std::chrono::steady_clock::now();
     double sec = std::chrono::duration<double>(t1 - t0).count();
     std::printf("labelled %lld seconds %.6f roots %zu threads %d\n", total,
                 sec, roots.size(), threads);
+    for (int k = 0; k < 64; k++)
+        if (g_units[k])
+            std::printf("group %d labelled %lld thread_seconds %.6f units %lld\n", k,
+                        g_lab[k], g_sec[k], g_units[k]);
     return 0;
 }

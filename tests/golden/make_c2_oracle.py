@@ -1,8 +1,15 @@
 """Full-size pins for the 4-clique / 4-cycle workload graph (R-MAT 2^20,
-2^24 samples, (a,b,c) = (.57,.19,.19), seed 2): the oracle's restatement of
-the reference engine (oracle/oracle.cpp, OpenMP) run over the whole graph on
-the host, root range by root range.  Writes tests/golden/c2_oracle.json.
-Takes about 45 minutes for the 4-clique on 8 threads; the 4-cycle is slower.
+2^24 samples, (a,b,c) = (.57,.19,.19), seed 2), computed on the host and
+written to tests/golden/c2_oracle.json:
+
+  k4      the oracle's restatement of the reference engine (oracle/oracle.cpp,
+          OpenMP) over the whole graph, root range by root range (about 45
+          minutes on 8 threads);
+  c4      the exact 4-cycle count by another route than the GPU's: wedges on
+          the graph's own ids, each cycle counted at its LARGEST vertex
+          (oracle_c4_rooted, at_largest = 1).  The GPU kernels count each
+          cycle at its smallest vertex of the degree-ordered copy, so the two
+          share neither the rooting nor the vertex ids.
 
     python tests/golden/make_c2_oracle.py [--threads 8] [--patterns k4,c4]
 """
@@ -47,6 +54,13 @@ def main() -> None:
     for name in a.patterns.split(","):
         p = PATTERNS[name]
         t0 = time.time()
+        if name == "c4":
+            tot = O.c4_rooted(off, adj, at_largest=True, threads=a.threads)
+            out[name] = {"pattern": p, "exact_at_largest_vertex": tot,
+                         "seconds": time.time() - t0, "threads": a.threads}
+            out_path.write_text(json.dumps(out, indent=1) + "\n")
+            print(name, tot, flush=True)
+            continue
         tot = 0
         for i in range(a.parts):
             st, c, _ = O.ref_engine(off, adj, sched[p], roots=(V * i // a.parts,

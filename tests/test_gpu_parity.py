@@ -287,7 +287,8 @@ def test_full_size_workload_graph_against_oracle(gat):
     """The bench's graph at full size (R-MAT 2^20, 2^24 samples, seed 2):
     GPU reference-compatible 4-clique = the oracle's restatement of the
     reference engine over the whole graph (tests/golden/c2_oracle.json,
-    made on the host by make_c2_oracle.py) = 4 x the GPU exact count."""
+    made on the host by make_c2_oracle.py) = 4 x the GPU exact count; GPU
+    exact 4-cycle = the host's whole-graph count by another rooting."""
     import json
     from pathlib import Path
 
@@ -301,9 +302,15 @@ def test_full_size_workload_graph_against_oracle(gat):
     ref = ex.count(g, gat.Schedule(k4["pattern"], "ref")).count
     assert ref == k4["ref_engine_oracle"]
     assert ref == 4 * exact
-    if "c4" in pins:
-        c4 = pins["c4"]
-        assert ex.count(g, gat.Schedule(c4["pattern"], "ref")).count == c4["ref_engine_oracle"]
+    # The 4-cycle: the wedge kernels (cycles rooted at their smallest vertex
+    # of the degree-ordered copy) and the plan path against the host count
+    # rooted at each cycle's largest vertex on the graph's own ids.
+    c4 = pins["c4"]
+    s = gat.Schedule(c4["pattern"], "exact")
+    assert ex.count(g, s).count == c4["exact_at_largest_vertex"]
+    plain = gat.Config.engine_default()
+    plain.special_kernels = 0
+    assert gat.Executor(plain).count(g, s).count == c4["exact_at_largest_vertex"]
 
 
 def test_schedule_variants_count_the_same(gat, oracle):

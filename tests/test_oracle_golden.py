@@ -92,3 +92,59 @@ def test_oracle_ref_engine_equals_reference_binary(oracle, golden_schedules, gol
         assert got == e["ref_engine_answer"], (e["graph"], e["pattern"], got)
         checked += 1
     assert checked >= 140
+
+
+def test_restricted_counts_of_exact_plans_match_reference_binary(gat, oracle, golden_naive,
+                                                                 golden_graphs):
+    """The full-size pins rest on this: for every exact plan, labelled
+    embeddings of the plan's vertex order under its order conditions, summed
+    over all roots and divided by the plan's divisor, give the reference
+    naive matcher's Answer / |Aut| on every golden graph."""
+    checked = 0
+    plans = {}
+    for e in golden_naive:
+        n = int(round(len(e["adj"]) ** 0.5))
+        if n < 3 or e["graph"] == "c1_er10000" and n > 3:
+            continue
+        if e["adj"] not in plans:
+            try:
+                d = gat.Schedule(e["adj"], "exact").dump()
+            except gat.GatError:
+                continue  # disconnected patterns have no exact plan
+            plans[e["adj"]] = (*oracle.plan_conditions(d), d["divisor"])
+        q, less, div = plans[e["adj"]]
+        off, adj = golden_graphs[e["graph"]].csr()
+        raw = oracle.restricted_labelled(off, adj, q, less)
+        assert raw % div == 0 and raw // div == e["naive_answer"] // oracle.automorphisms(e["adj"]), e
+        checked += 1
+    assert checked > 250
+
+
+def test_c4_rooted_counts_match_reference_binary(oracle, golden_naive, golden_graphs):
+    """4-cycles counted at their smallest and at their largest vertex both
+    give naive_pm's Answer / 8, and root ranges add up."""
+    seen = 0
+    for e in golden_naive:
+        if e["adj"] != "0101101001011010":
+            continue
+        off, adj = golden_graphs[e["graph"]].csr()
+        want = e["naive_answer"] // 8
+        assert oracle.c4_rooted(off, adj) == want
+        assert oracle.c4_rooted(off, adj, at_largest=True) == want
+        V = len(off) - 1
+        cuts = [0, V // 3, V // 2, V]
+        assert sum(oracle.c4_rooted(off, adj, roots=(a, b))
+                   for a, b in zip(cuts, cuts[1:])) == want
+        seen += 1
+    assert seen >= 5
+
+
+def test_degree_order_restatement(gat, oracle, golden_graphs):
+    """The oracle's relabel (decreasing degree, ties by id) is a relabelling:
+    same degree sequence sorted, same counts."""
+    off, adj = golden_graphs["ba60"].csr()
+    no, na = oracle.degree_order(off, adj)
+    deg = np.diff(off)
+    assert (np.diff(no) == np.sort(deg)[::-1]).all()
+    for p in ("011101110", "0101101001011010", "0100110110010110110010100"):
+        assert oracle.exact_count(no, na, p) == oracle.exact_count(off, adj, p)

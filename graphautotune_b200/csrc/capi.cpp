@@ -713,116 +713,64 @@ void gat_executor_free(gat_executor *e) { delete e; }
 
 namespace {
 
-// The exact 4-cycle count through the wedge-aggregation kernels: counter
-// rows for light tiles and heavy batches in scratch, kept all-zero between
-// launches.
+// The exact 4-cycle count through the wedge-aggregation kernels (cycles.cu):
+// per-root counts are tallied in shared memory, so the scratch is only the
+// deferred-root list and the root kernel's list cursors.
 int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t vb,
            int64_t ve, LaunchShape shape, cudaStream_t strm, bool balg, uint64_t *count,
            gat_stats *stats, std::chrono::steady_clock::time_point t0) {
-    const int occ = c4_blocks_per_sm(shape.tile, shape.block, balg);
-    const int hocc = c4_heavy_blocks_per_sm(balg);
-    if (occ <= 0 || hocc <= 0) return fail(GAT_ERR_CUDA, "4-cycle kernels do not fit on the device");
-    const int64_t V = std::max<int64_t>(view.V, 1);
+    const bool wide = view.max_degree >= 65536;
+    const int locc = c4_light_blocks_per_sm(balg);
+    const int rocc = c4_root_blocks_per_sm(wide, balg);
+    if (locc <= 0 || rocc <= 0) return fail(GAT_ERR_CUDA, "4-cycle kernels do not fit on the device");
     // Heavy roots: the leading run of ids with degree >= kC4HeavyDegree (on a
-    // degree-ordered copy, exactly the vertices of that degree).
+    // degree-ordered copy, exactly the vertices of that degree) take a CTA
+    // each from the start.
     constexpr int64_t kC4HeavyDegree = 256;
     int64_t H = 0;
     while (H < view.V && dc.off_host[H + 1] - dc.off_host[H] >= kC4HeavyDegree) H++;
-    const int64_t words = (V + 1023) / 1024;  // line bitmap: one bit per 32 counters
-    const int64_t budget = e->cfg.memory_budget > 0 ? e->cfg.memory_budget : (int64_t(16) << 30);
-    const int64_t tiles_per_block = shape.block / shape.tile;
-    const int64_t row_bytes = V * 4;
-    // Half the budget for heavy batches; light tiles' rows get the other half,
-    // at most 4 GiB (with one-lane tiles every thread holds a row).
-    const int64_t light_budget = std::min<int64_t>(budget / 2, int64_t(4) << 30);
-    int64_t light_grid = e->cfg.num_blocks > 0 ? e->cfg.num_blocks : (int64_t)e->sms * occ;
-    light_grid = std::min<int64_t>(light_grid, light_budget / (tiles_per_block * row_bytes));
-    const int64_t heavy_row = row_bytes + words * 4;
-    int64_t R = std::min<int64_t>(std::max<int64_t>(H, 1), (budget / 2) / heavy_row);
-    if (light_grid < 1 || R < 1)
-        return fail(GAT_ERR_MEMORY, "memory budget below the 4-cycle counters' minimum");
-    // Every region starts on a 256-byte boundary (rows are V words, which for
-    // odd V would leave the 8-byte arrays after them misaligned).
+    const int light_grid = e->sms * locc;
+    const int root_grid = e->cfg.num_blocks > 0 ? std::min(e->cfg.num_blocks, e->sms * rocc)
+                                                : e->sms * rocc;
+    const int64_t stride = std::max<int64_t>(view.max_degree, 1);
     auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
-    const int64_t light_bytes = al(light_grid * tiles_per_block * row_bytes);
-    const int64_t hrows_bytes = al(R * row_bytes);
-    const int64_t bms_bytes = al(R * words * 4);
-    // the largest number of (root, upper neighbour) units in one heavy batch
-    int64_t max_units = 0;
-    {
-        auto up = [&](int64_t v) { return dc.off_host[v] - dc.lo_host[v]; };
-        const int64_t he = std::min(ve, H);
-        for (int64_t r0 = vb; r0 < he; r0 += R)
-            max_units = std::max(max_units, up(std::min(r0 + R, he)) - up(r0));
-    }
-    const int64_t np_bytes = al((max_units + 1) * 4);
-    const int64_t pref_bytes = al((max_units + 1) * 8);
-    const int64_t temp_bytes = al((int64_t)c4_scan_temp_bytes(max_units + 1));
-    const size_t need = size_t(light_bytes + hrows_bytes + bms_bytes + np_bytes + pref_bytes +
-                               temp_bytes);
+    const int64_t aux_bytes = al(sizeof(C4Aux));
+    const int64_t def_bytes = al(std::max<int64_t>(view.V, 1) * 4);
+    const int64_t cur_bytes = al(int64_t(root_grid) * stride * 4);
+    const size_t need = size_t(aux_bytes + def_bytes + cur_bytes);
     cudaError_t ce;
     if (need > e->scratch_bytes) {
         cudaFree(e->scratch);
         e->scratch = nullptr;
         e->scratch_bytes = 0;
         if ((ce = cudaMalloc(&e->scratch, need)) != cudaSuccess)
-            return fail(GAT_ERR_MEMORY, std::string("counter allocation: ") + cudaGetErrorString(ce));
+            return fail(GAT_ERR_MEMORY, std::string("4-cycle scratch: ") + cudaGetErrorString(ce));
         e->scratch_bytes = need;
-        e->scratch_clean = false;
     }
-    if (!e->scratch_clean) {
-        if ((ce = cudaMemsetAsync(e->scratch, 0, e->scratch_bytes, strm)) != cudaSuccess)
-            return cuda_fail(ce, "counter clear");
-        e->scratch_clean = true;
-    }
+    e->scratch_clean = false;
     unsigned char *base = reinterpret_cast<unsigned char *>(e->scratch);
     C4Launch L;
     L.g = view;
-    L.off_host = dc.off_host.data();
-    L.lo_host = dc.lo_host.data();
     L.v_begin = vb;
     L.v_end = ve;
     L.heavy_end = H;
-    L.tile = shape.tile;
-    L.block = shape.block;
-    L.chunk = shape.chunk;
-    L.light_grid = (int)light_grid;
-    L.heavy_grid = e->sms * hocc;
+    L.light_grid = light_grid;
+    L.root_grid = root_grid;
     L.ctr = e->ctr;
-    L.stride = V;
-    L.light_rows = reinterpret_cast<uint32_t *>(base);
-    L.heavy_rows = reinterpret_cast<uint32_t *>(base + light_bytes);
-    L.heavy_bms = reinterpret_cast<uint32_t *>(base + light_bytes + hrows_bytes);
-    unsigned char *tail = base + light_bytes + hrows_bytes + bms_bytes;
-    L.npieces = reinterpret_cast<int32_t *>(tail);
-    L.pieces_pref = reinterpret_cast<int64_t *>(tail + np_bytes);
-    L.scan_temp = tail + np_bytes + pref_bytes;
-    L.scan_temp_bytes = (size_t)temp_bytes;
-    L.rows_per_batch = R;
-    L.words = words;
+    L.aux = reinterpret_cast<C4Aux *>(base);
+    L.deferred = reinterpret_cast<int32_t *>(base + aux_bytes);
+    L.cursors = reinterpret_cast<int32_t *>(base + aux_bytes + def_bytes);
+    L.cursor_stride = stride;
     L.stats = balg;
-    shape.grid = (int)light_grid;
     cudaEventRecord(e->ev0, strm);
     ce = launch_c4(L, strm);
-    if (ce != cudaSuccess) {
-        e->scratch_clean = false;
-        return cuda_fail(ce, "4-cycle launch");
-    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "4-cycle launch");
     cudaEventRecord(e->ev1, strm);
-    // Counter rows and bitmaps are zero again; clear the piece arrays and the
-    // scan's temp storage too, so the whole scratch stays zero for the next
-    // count, whose layout may differ.
-    if ((ce = cudaMemsetAsync(tail, 0, size_t(np_bytes + pref_bytes + temp_bytes), strm)) !=
-        cudaSuccess) {
-        e->scratch_clean = false;
-        return cuda_fail(ce, "4-cycle scratch clear");
-    }
     if ((ce = cudaMemcpyAsync(e->host_ctr, e->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
                               strm)) != cudaSuccess ||
-        (ce = cudaStreamSynchronize(strm)) != cudaSuccess) {
-        e->scratch_clean = false;
+        (ce = cudaStreamSynchronize(strm)) != cudaSuccess)
         return cuda_fail(ce, "4-cycle count");
-    }
+    if (e->host_ctr->error) return fail(GAT_ERR_DEVICE, "4-cycle kernel reported an internal error");
     float ms = 0;
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
     const int64_t raw = (int64_t)e->host_ctr->result;
@@ -833,11 +781,10 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
     st.divisor = 1;
     st.tasks = (uint64_t)(ve - vb);
     st.balg_bytes = e->host_ctr->bytes;
-    st.grid = shape.grid;
-    st.block = shape.block;
+    st.grid = root_grid;
+    st.block = 1024;
     st.tile = shape.tile;
-    const int64_t hb = std::min(ve, H) > vb ? (std::min(ve, H) - vb + R - 1) / R : 0;
-    st.launches = (std::max(vb, H) < ve ? 1 : 0) + 3 * hb;  // + one scan per batch
+    st.launches = (std::max(vb, H) < ve ? 1 : 0) + 1;
     st.scratch_bytes = (int64_t)need;
     st.total_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

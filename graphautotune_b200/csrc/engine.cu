@@ -822,341 +822,6 @@ __global__ void __launch_bounds__(256)
     if (t.lane == 0 && cur_job >= 0 && acc) atomicAdd(&results[cur_job], acc);
 }
 
-// Exact 4-cycle count by wedge aggregation.  Every 4-cycle is counted once,
-// at its smallest vertex v0 together with the vertex x opposite v0: its other
-// two vertices are common neighbours of v0 and x above v0.  So
-//   count = sum_{v0} sum_{x > v0} C(c(v0, x), 2),
-//   c(v0, x) = |{ v1 in N(v0) : v1 > v0, x in N(v1) }|   (x > v0 too).
-// On the degree-ordered copy (id 0 = largest degree) v0 is the cycle's
-// highest-degree vertex and v1 has degree <= deg(v0), so the wedges number
-// at most sum over edges of the smaller endpoint's degree, instead of
-// sum_v deg(v)^2 with the opposite orientation.
-//
-// The counters c(v0, .) are a V-word row that is all zero between roots:
-// pass 1 adds 1 to row[x] for every wedge v0 - v1 - x and notes where it
-// wrote; pass 2 reads each noted counter once, adds C(c, 2) and writes the
-// word back to zero.
-//
-//  * Light roots (degree below the heavy threshold) take one tile each, a
-//    private row in scratch and a list of first touches in shared memory (if
-//    the list overflows, pass 2 walks the wedges again with an atomic
-//    exchange).
-//  * Heavy roots (the leading run of ids with large degree) are spread over
-//    the whole grid: a batch of R roots has R shared rows with line bitmaps
-//    in scratch; pass 1 hands out the (v0, v1) pairs of the batch through the
-//    cursor (in root order, so the rows in use at any time stay in L2) and
-//    increments counters with fire-and-forget atomics; a separate pass-2
-//    launch visits the marked lines.
-// Kernels of one count are ordered on the stream; none waits on another CTA.
-
-
-// First index i of the sorted a[0, n) with a[i] > x (one lane alone).
-__device__ __forceinline__ int upper_serial(const int32_t *a, int n, int32_t x) {
-    int lo = 0;
-    while (n > 0) {
-        const int h = n >> 1;
-        const bool right = a[lo + h] <= x;
-        lo = right ? lo + h + 1 : lo;
-        n = right ? n - h - 1 : h;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ unsigned long long pairs_of(unsigned c) {
-    return (unsigned long long)c * (c - 1) / 2;
-}
-
-template <int G, bool STATS>
-__global__ void __launch_bounds__(256)
-    c4_light_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
-                    const int64_t *__restrict__ lo_off, int64_t v_begin, int64_t v_end,
-                    int32_t chunk, DevCounters *ctr, uint32_t *cnt_all, int64_t cnt_stride) {
-    // 32 KB of touched lists per block whatever the tile width.
-    constexpr int kC4LightList = 32 * G;
-    __shared__ int32_t lists[256 / G][kC4LightList];
-    __shared__ int32_t lens[256 / G];
-    const Tile<G> t;
-    const int tiles_per_block = blockDim.x / G;
-    const int tib = threadIdx.x / G;
-    int32_t *list = lists[tib];
-    uint32_t *cnt = cnt_all + ((int64_t)blockIdx.x * tiles_per_block + tib) * cnt_stride;
-    unsigned long long part = 0, bytes = 0;
-    for (;;) {
-        unsigned long long s = 0;
-        if (t.lane == 0)
-            s = (unsigned long long)v_begin + atomicAdd(&ctr->cursor, (unsigned long long)chunk);
-        s = t.bcast(s, 0);
-        if (s >= (unsigned long long)v_end) break;
-        const int64_t e = min((int64_t)s + chunk, v_end);
-        for (int64_t v0 = (int64_t)s; v0 < e; v0++) {
-            const int64_t o0 = off[v0];
-            const int32_t d0 = (int32_t)(off[v0 + 1] - o0);
-            const int32_t lo0 = (int32_t)(lo_off[v0 + 1] - lo_off[v0]);
-            if (d0 - lo0 < 2) continue;  // a cycle needs two neighbours above v0
-            if (t.lane == 0) lens[tib] = 0;
-            t.sync();
-            // pass 1: lane per upper neighbour v1
-            for (int i = lo0 + t.lane; i < d0; i += G) {
-                const int32_t v1 = adj[o0 + i];
-                const int64_t o1 = off[v1];
-                const int32_t d1 = (int32_t)(off[v1 + 1] - o1);
-                const int32_t *n1 = adj + o1;
-                for (int k = upper_serial(n1, d1, (int32_t)v0); k < d1; k++) {
-                    const int32_t x = n1[k];
-                    if (atomicAdd(&cnt[x], 1u) == 0u) {
-                        const int p = atomicAdd(&lens[tib], 1);
-                        if (p < kC4LightList) list[p] = x;
-                    }
-                    if (STATS) bytes += 12;
-                }
-            }
-            t.sync();
-            const int L = lens[tib];
-            if (L <= kC4LightList) {
-                for (int j = t.lane; j < L; j += G) {
-                    const int32_t x = list[j];
-                    const uint32_t c = cnt[x];
-                    cnt[x] = 0u;
-                    part += pairs_of(c);
-                }
-                if (STATS) bytes += 8ull * (unsigned)L;
-            } else {
-                for (int i = lo0 + t.lane; i < d0; i += G) {
-                    const int32_t v1 = adj[o0 + i];
-                    const int64_t o1 = off[v1];
-                    const int32_t d1 = (int32_t)(off[v1 + 1] - o1);
-                    const int32_t *n1 = adj + o1;
-                    for (int k = upper_serial(n1, d1, (int32_t)v0); k < d1; k++)
-                        part += pairs_of(atomicExch(&cnt[n1[k]], 0u));
-                }
-            }
-            t.sync();
-        }
-    }
-    part = t.sum(part);
-    if (STATS) bytes = t.sum(bytes);
-    if (t.lane == 0) {
-        atomicAdd(&ctr->result, part);
-        if (STATS) atomicAdd(&ctr->bytes, bytes);
-    }
-}
-
-// Heavy rows carry a line bitmap: bit (x >> 5) of the row's bitmap is set
-// when any counter of the 32-word line holding x was incremented.  Pass 1
-// increments counters with fire-and-forget atomics (no value comes back, so
-// no round trip stalls the warp) and sets line bits, batching the bits of one
-// bitmap word per lane and skipping the atomic when a plain read already
-// shows them; pass 2 visits only the marked lines.
-struct LineMarks {
-    uint32_t *bm = nullptr;
-    int64_t w = -1;
-    uint32_t bits = 0;
-    __device__ __forceinline__ void flush() {
-        if (bits && (bm[w] & bits) != bits) atomicOr(&bm[w], bits);
-        bits = 0;
-    }
-    __device__ __forceinline__ void mark(uint32_t *row_bm, int32_t x) {
-        const int64_t wi = x >> 10;
-        if (row_bm != bm || wi != w) {
-            if (bm) flush();
-            bm = row_bm;
-            w = wi;
-        }
-        bits |= 1u << ((x >> 5) & 31);
-    }
-};
-
-constexpr int kC4Piece = 1024;  // entries of a long list per pass-1b piece
-
-// Root of unit tu among [r0, r1): the largest v with up(v) <= tu.
-__device__ __forceinline__ int64_t c4_root_of(const int64_t *off, const int64_t *lo_off,
-                                              int64_t r0, int64_t r1, int64_t tu) {
-    int64_t lo = r0, n = r1 - r0;
-    while (n > 0) {
-        const int64_t h = n >> 1;
-        const int64_t m = lo + h;
-        const bool right = off[m + 1] - lo_off[m + 1] <= tu;
-        lo = right ? m + 1 : lo;
-        n = right ? n - h - 1 : h;
-    }
-    return min(lo, r1 - 1);
-}
-
-// Pass 1a over heavy roots [r0, r1): the units are the pairs (v0, v1 > v0),
-// numbered by up(v) = off[v] - lo_off[v] (upper neighbours before v).  A warp
-// takes `chunk` consecutive units; each lane resolves its own and walks its
-// list above v0 alone when it is short (< 64 entries).  A long list (a hub
-// neighbour) is not walked here: the lane records how many kC4Piece-entry
-// pieces it has, and pass 1b spreads those pieces over the whole grid, so no
-// warp is left alone with a list of ~10^4 entries.
-template <bool STATS>
-__global__ void __launch_bounds__(256)
-    c4_heavy_pass1_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
-                          const int64_t *__restrict__ lo_off, int64_t r0, int64_t r1,
-                          int64_t u_begin, int64_t u_end, int32_t chunk, DevCounters *ctr,
-                          uint32_t *rows, uint32_t *bms, int64_t stride, int64_t words,
-                          int32_t *npieces) {
-    const int lane = threadIdx.x & 31;
-    unsigned long long bytes = 0;
-    LineMarks marks;
-    for (;;) {
-        unsigned long long s = 0;
-        if (lane == 0) s = (unsigned long long)u_begin + atomicAdd(&ctr->cursor, (unsigned long long)chunk);
-        s = __shfl_sync(0xffffffffu, s, 0);
-        if (s >= (unsigned long long)u_end) break;
-        const int64_t e = min((int64_t)s + chunk, u_end);
-        int64_t v0 = c4_root_of(off, lo_off, r0, r1, (int64_t)s + lane);
-        for (int64_t base = (int64_t)s; base < e; base += 32) {
-            const int64_t tu = base + lane;
-            const bool live = tu < e;
-            int32_t s1 = 0, d1 = 0, row = 0;
-            int64_t o1 = 0;
-            if (live) {
-                while (off[v0 + 1] - lo_off[v0 + 1] <= tu) v0++;
-                const int64_t j = tu - (off[v0] - lo_off[v0]);
-                const int32_t lo0 = (int32_t)(lo_off[v0 + 1] - lo_off[v0]);
-                const int32_t v1 = adj[off[v0] + lo0 + j];
-                o1 = off[v1];
-                d1 = (int32_t)(off[v1 + 1] - o1);
-                s1 = upper_serial(adj + o1, d1, (int32_t)v0);
-                row = (int32_t)(v0 - r0);
-            }
-            const bool longl = live && d1 - s1 >= 64;
-            if (live && !longl) {
-                uint32_t *rw = rows + (int64_t)row * stride;
-                uint32_t *bm = bms + (int64_t)row * words;
-                for (int k = s1; k < d1; k++) {
-                    const int32_t x = adj[o1 + k];
-                    atomicAdd(&rw[x], 1u);
-                    marks.mark(bm, x);
-                }
-                if (STATS) bytes += 12ull * (unsigned)(d1 - s1);
-            }
-            // long lists become pieces for pass 1b
-            if (live) npieces[tu - u_begin] = longl ? (d1 - s1 + kC4Piece - 1) / kC4Piece : 0;
-        }
-    }
-    if (marks.bm) marks.flush();
-    if (STATS) {
-        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
-        if (lane == 0) atomicAdd(&ctr->bytes, bytes);
-    }
-}
-
-// Pass 1b: the pieces of the long lists, pref[u] = pieces of units before u
-// (u counted from u_begin; pref[n_units] = all pieces).  A warp takes one
-// piece from the cursor, re-derives its unit (root, neighbour, start of the
-// list above the root) and adds its up to kC4Piece wedges.
-template <bool STATS>
-__global__ void __launch_bounds__(256)
-    c4_heavy_pass1b_kernel(const int64_t *__restrict__ off, const int32_t *__restrict__ adj,
-                           const int64_t *__restrict__ lo_off, int64_t r0, int64_t r1,
-                           int64_t u_begin, const int64_t *__restrict__ pref, int64_t n_units,
-                           DevCounters *ctr, uint32_t *rows, uint32_t *bms, int64_t stride,
-                           int64_t words) {
-    const int lane = threadIdx.x & 31;
-    const int64_t total = pref[n_units];
-    unsigned long long bytes = 0;
-    LineMarks marks;
-    for (;;) {
-        unsigned long long q = 0;
-        if (lane == 0) q = atomicAdd(&ctr->cursor, 1ull);
-        q = __shfl_sync(0xffffffffu, q, 0);
-        if ((int64_t)q >= total) break;
-        int64_t lo = 0, n = n_units;  // unit: last u with pref[u] <= q
-        while (n > 0) {
-            const int64_t h = n >> 1;
-            const bool right = pref[lo + h + 1] <= (int64_t)q;
-            lo = right ? lo + h + 1 : lo;
-            n = right ? n - h - 1 : h;
-        }
-        const int64_t tu = u_begin + lo;
-        const int64_t v0 = c4_root_of(off, lo_off, r0, r1, tu);
-        const int64_t j = tu - (off[v0] - lo_off[v0]);
-        const int32_t lo0 = (int32_t)(lo_off[v0 + 1] - lo_off[v0]);
-        const int32_t v1 = adj[off[v0] + lo0 + j];
-        const int64_t o1 = off[v1];
-        const int32_t d1 = (int32_t)(off[v1 + 1] - o1);
-        const int32_t s1 = upper_serial(adj + o1, d1, (int32_t)v0);
-        const int32_t b = s1 + (int32_t)((int64_t)q - pref[lo]) * kC4Piece;
-        const int32_t e = min(d1, b + kC4Piece);
-        uint32_t *rw = rows + (v0 - r0) * stride;
-        uint32_t *bm = bms + (v0 - r0) * words;
-        for (int k = b + lane; k < e; k += 32) {
-            const int32_t x = adj[o1 + k];
-            atomicAdd(&rw[x], 1u);
-            marks.mark(bm, x);
-        }
-        if (STATS && lane == 0) bytes += 12ull * (unsigned)(e - b);
-    }
-    if (marks.bm) marks.flush();
-    if (STATS) {
-        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
-        if (lane == 0) atomicAdd(&ctr->bytes, bytes);
-    }
-}
-
-// Pass 2 over the R rows of a batch: a warp takes 32 bitmap words of one row
-// (1,024 lines), clears them, and for every marked line reads its 32 counters
-// in one coalesced access, adds C(c, 2) for each and writes the non-zero ones
-// back to zero.
-template <bool STATS>
-__global__ void __launch_bounds__(256)
-    c4_heavy_pass2_kernel(int32_t R, int64_t V, uint32_t *rows, uint32_t *bms, int64_t stride,
-                          int64_t words, DevCounters *ctr) {
-    __shared__ unsigned long long red[8];
-    const int lane = threadIdx.x & 31;
-    const int64_t groups = (words + 31) / 32;
-    const int64_t total = (int64_t)R * groups;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    unsigned long long part = 0, bytes = 0;
-    for (int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; gw < total;
-         gw += nwarps) {
-        const int64_t r = gw / groups, wg = (gw % groups) * 32;
-        uint32_t *bm = bms + r * words;
-        uint32_t *rw = rows + r * stride;
-        const int64_t wi = wg + lane;
-        uint32_t word = 0;
-        if (wi < words) {
-            word = bm[wi];
-            if (word) bm[wi] = 0u;
-        }
-        if (STATS) bytes += 4;
-        unsigned todo = __ballot_sync(0xffffffffu, word != 0u);
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            uint32_t w = __shfl_sync(0xffffffffu, word, src);
-            const int64_t line0 = (wg + src) * 32;
-            while (w) {
-                const int b = __ffs(w) - 1;
-                w &= w - 1;
-                const int64_t x = (line0 + b) * 32 + lane;
-                if (x < V) {
-                    const uint32_t c = rw[x];
-                    if (c) {
-                        rw[x] = 0u;
-                        part += pairs_of(c);
-                    }
-                }
-                if (STATS) bytes += 8;
-            }
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        part += __shfl_xor_sync(0xffffffffu, part, o);
-        if (STATS) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
-    }
-    if (lane == 0) red[threadIdx.x >> 5] = part;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long t = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += red[i];
-        atomicAdd(&ctr->result, t);
-    }
-    if (STATS && lane == 0) atomicAdd(&ctr->bytes, bytes);
-}
-
 template <int G, bool STATS>
 cudaError_t launch_one(const SearchArgs &a, int grid, int block,
                        cudaStream_t stream) {
@@ -1278,128 +943,6 @@ int batch_occ(int block) {
     return n;
 }
 }  // namespace
-
-namespace {
-template <int G, bool STATS>
-int c4_occ(int block) {
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, c4_light_kernel<G, STATS>, block, 0) !=
-        cudaSuccess)
-        return 0;
-    return n;
-}
-
-template <bool STATS>
-int c4_heavy_occ() {
-    int a = 0, b = 0;
-    int c = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, c4_heavy_pass1_kernel<STATS>, 256,
-                                                      0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, c4_heavy_pass2_kernel<STATS>, 256,
-                                                      0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, c4_heavy_pass1b_kernel<STATS>, 256,
-                                                      0) != cudaSuccess)
-        return 0;
-    return min(min(a, b), c);
-}
-}  // namespace
-
-int c4_blocks_per_sm(int tile, int block, bool stats) {
-#define GAT_C4O(G) return stats ? c4_occ<G, true>(block) : c4_occ<G, false>(block)
-    switch (tile) {
-        case 1: GAT_C4O(1);
-        case 2: GAT_C4O(2);
-        case 4: GAT_C4O(4);
-        case 8: GAT_C4O(8);
-        case 16: GAT_C4O(16);
-        case 32: GAT_C4O(32);
-        default: return 0;
-    }
-#undef GAT_C4O
-}
-
-int c4_heavy_blocks_per_sm(bool stats) {
-    return stats ? c4_heavy_occ<true>() : c4_heavy_occ<false>();
-}
-
-size_t c4_scan_temp_bytes(int64_t n) {
-    size_t b = 0;
-    if (cub::DeviceScan::ExclusiveSum(nullptr, b, (const int32_t *)nullptr, (int64_t *)nullptr,
-                                      (int)std::max<int64_t>(n, 1)) != cudaSuccess)
-        return 0;
-    return b;
-}
-
-cudaError_t launch_c4(const C4Launch &L, cudaStream_t st) {
-    const DevGraphView &g = L.g;
-    DevCounters *ctr = L.ctr;
-    cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(DevCounters), st);
-    if (e != cudaSuccess) return e;
-    const int ch = L.chunk > 0 ? L.chunk : 1;
-    const int64_t lb = std::max(L.v_begin, L.heavy_end), le = L.v_end;
-    if (lb < le) {
-#define GAT_C4L(G)                                                                             \
-    if (L.stats)                                                                               \
-        c4_light_kernel<G, true><<<L.light_grid, L.block, 0, st>>>(                            \
-            g.off, g.adj, g.lo_off, lb, le, ch, ctr, L.light_rows, L.stride);                  \
-    else                                                                                       \
-        c4_light_kernel<G, false><<<L.light_grid, L.block, 0, st>>>(                           \
-            g.off, g.adj, g.lo_off, lb, le, ch, ctr, L.light_rows, L.stride);                  \
-    break
-        switch (L.tile) {
-            case 1: GAT_C4L(1);
-            case 2: GAT_C4L(2);
-            case 4: GAT_C4L(4);
-            case 8: GAT_C4L(8);
-            case 16: GAT_C4L(16);
-            case 32: GAT_C4L(32);
-            default: return cudaErrorInvalidValue;
-        }
-#undef GAT_C4L
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
-    const int64_t he = std::min(L.v_end, L.heavy_end);
-    auto up = [&](int64_t v) { return L.off_host[v] - L.lo_host[v]; };
-    for (int64_t r0 = L.v_begin; r0 < he; r0 += L.rows_per_batch) {
-        const int64_t r1 = std::min(r0 + L.rows_per_batch, he);
-        const int32_t R = (int32_t)(r1 - r0);
-        const int64_t u0 = up(r0), n_units = up(r1) - u0;
-        if ((e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess ||
-            (e = cudaMemsetAsync(L.npieces + n_units, 0, sizeof(int32_t), st)) != cudaSuccess)
-            return e;
-        if (L.stats)
-            c4_heavy_pass1_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
-                g.off, g.adj, g.lo_off, r0, r1, u0, u0 + n_units, 128, ctr, L.heavy_rows,
-                L.heavy_bms, L.stride, L.words, L.npieces);
-        else
-            c4_heavy_pass1_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
-                g.off, g.adj, g.lo_off, r0, r1, u0, u0 + n_units, 128, ctr, L.heavy_rows,
-                L.heavy_bms, L.stride, L.words, L.npieces);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        size_t tb = L.scan_temp_bytes;
-        if ((e = cub::DeviceScan::ExclusiveSum(L.scan_temp, tb, L.npieces, L.pieces_pref,
-                                               (int)(n_units + 1), st)) != cudaSuccess ||
-            (e = cudaMemsetAsync(&ctr->cursor, 0, sizeof(ctr->cursor), st)) != cudaSuccess)
-            return e;
-        if (L.stats)
-            c4_heavy_pass1b_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
-                g.off, g.adj, g.lo_off, r0, r1, u0, L.pieces_pref, n_units, ctr,
-                L.heavy_rows, L.heavy_bms, L.stride, L.words);
-        else
-            c4_heavy_pass1b_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
-                g.off, g.adj, g.lo_off, r0, r1, u0, L.pieces_pref, n_units, ctr,
-                L.heavy_rows, L.heavy_bms, L.stride, L.words);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if (L.stats)
-            c4_heavy_pass2_kernel<true><<<L.heavy_grid, 256, 0, st>>>(
-                R, g.V, L.heavy_rows, L.heavy_bms, L.stride, L.words, ctr);
-        else
-            c4_heavy_pass2_kernel<false><<<L.heavy_grid, 256, 0, st>>>(
-                R, g.V, L.heavy_rows, L.heavy_bms, L.stride, L.words, ctr);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
-    return cudaSuccess;
-}
 
 int batch_blocks_per_sm(int tile, int block) {
     switch (tile) {

@@ -66,34 +66,28 @@ struct DevCounters {
 };
 
 // Exact 4-cycle count by wedge aggregation over smallest vertices
-// [v_begin, v_end) (plans with special == GAT_SPECIAL_C4).  Roots below
-// heavy_end are spread over the grid in batches of rows_per_batch (shared
-// counter rows, each with a line bitmap of `words` words); the others take
-// one tile each with a private row (light_grid x block/tile rows).  Every
-// row has `stride` words; rows and bitmaps must be zero before the launch
-// and are zero again after it.
+// [v_begin, v_end) (plans with special == GAT_SPECIAL_C4), tallied in shared
+// memory (cycles.cu).  Roots below heavy_end take a CTA each; the others a
+// warp each, which defers roots with many wedges to the CTA kernel.
+struct C4Aux {
+    unsigned long long light_cursor;
+    unsigned long long deferred_count;
+    unsigned long long root_cursor;
+    unsigned long long pad;
+};
 struct C4Launch {
     DevGraphView g;
-    const int64_t *off_host = nullptr;  // host copies of off and lo_off
-    const int64_t *lo_host = nullptr;
     int64_t v_begin = 0, v_end = 0, heavy_end = 0;
-    int tile = 32, block = 256, chunk = 8, light_grid = 0, heavy_grid = 0;
+    int light_grid = 0, root_grid = 0;
     DevCounters *ctr = nullptr;
-    int64_t stride = 0;
-    uint32_t *light_rows = nullptr;
-    uint32_t *heavy_rows = nullptr;
-    uint32_t *heavy_bms = nullptr;
-    int64_t rows_per_batch = 1, words = 0;
-    int32_t *npieces = nullptr;       // per unit of a batch (+1), long-list pieces
-    int64_t *pieces_pref = nullptr;   // their exclusive prefix (+1)
-    void *scan_temp = nullptr;
-    size_t scan_temp_bytes = 0;
+    C4Aux *aux = nullptr;
+    int32_t *deferred = nullptr;   // room for every light root
+    int32_t *cursors = nullptr;    // root_grid x cursor_stride list positions
+    int64_t cursor_stride = 0;     // >= the largest degree
     bool stats = false;
 };
-int c4_blocks_per_sm(int tile, int block, bool stats);
-int c4_heavy_blocks_per_sm(bool stats);
-// Temp storage of the piece scan over up to n units.
-size_t c4_scan_temp_bytes(int64_t n);
+int c4_light_blocks_per_sm(bool stats);
+int c4_root_blocks_per_sm(bool wide, bool stats);
 cudaError_t launch_c4(const C4Launch &launch, cudaStream_t st);
 
 // Batched launches: host code fills an array of batch_job_bytes()-sized job
@@ -123,6 +117,7 @@ int count_noalloc(const GatPlan &plan, const int64_t *d_off, const int32_t *d_ad
 
 enum : unsigned long long {
     GAT_DEVERR_SCRATCH = 1ull,  // a stored set would overflow its slot
+    GAT_DEVERR_TABLE = 2ull,    // a shared-memory count table ran out of slots
 };
 
 // Shared memory one tile needs.

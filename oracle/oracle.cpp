@@ -8,6 +8,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -286,6 +287,20 @@ struct Restricted {
     int upper[10][10];  // upper[k] = earlier b with f(k) < f(b)
     int nupper[10] = {};
     int32_t f[10];
+    // Work cap: candidates examined, charged to a shared budget in blocks;
+    // once it runs out every call returns at once and `over` is set.
+    std::atomic<int64_t> *budget = nullptr;
+    std::atomic<int> *over = nullptr;
+    int64_t local = 0;
+    bool charge(int64_t n) {
+        if (!budget) return true;
+        local += n;
+        if (local >= 4096) {
+            if (budget->fetch_sub(local) - local < 0) over->store(1);
+            local = 0;
+        }
+        return over->load(std::memory_order_relaxed) == 0;
+    }
     Restricted(const CSR &g_, const Pat &p_, const int32_t *less, int32_t nless)
         : g(g_), p(p_) {
         for (int i = 0; i < nless; i++) {
@@ -317,6 +332,7 @@ struct Restricted {
             e = b + all.size();
         }
         uint64_t n = 0;
+        if (!charge(e - b)) return 0;
         for (const int32_t *it = b; it < e; ++it) {
             const int32_t x = *it;
             bool ok = true;
@@ -539,6 +555,16 @@ uint64_t oracle_restricted_labelled(int32_t V, const int64_t *offs, const int32_
                                     const char *pattern, const int32_t *less,
                                     int32_t nless, int32_t root_begin, int32_t root_end,
                                     int threads) {
+    return oracle_restricted_labelled_capped(V, offs, adj, pattern, less, nless, root_begin,
+                                             root_end, threads, -1, nullptr);
+}
+
+uint64_t oracle_restricted_labelled_capped(int32_t V, const int64_t *offs,
+                                           const int32_t *adj, const char *pattern,
+                                           const int32_t *less, int32_t nless,
+                                           int32_t root_begin, int32_t root_end, int threads,
+                                           int64_t max_work, int *over) {
+    if (over) *over = 0;
     Pat p(pattern);
     if (p.n < 2 || nless < 0) return 0;
     for (int i = 0; i < 2 * nless; i++)
@@ -557,9 +583,15 @@ uint64_t oracle_restricted_labelled(int32_t V, const int64_t *offs, const int32_
         start[v - root_begin + 1] = start[v - root_begin] + (by_edge ? g.deg(v) : 1);
     const int64_t units = start.back();
     uint64_t total = 0;
+    std::atomic<int64_t> budget{max_work};
+    std::atomic<int> exceeded{0};
 #pragma omp parallel num_threads(threads) reduction(+ : total)
     {
         Restricted r(g, p, less, nless);
+        if (max_work >= 0) {
+            r.budget = &budget;
+            r.over = &exceeded;
+        }
         int32_t row = root_begin;
 #pragma omp for schedule(dynamic, 256)
         for (int64_t u = 0; u < units; u++) {
@@ -584,7 +616,8 @@ uint64_t oracle_restricted_labelled(int32_t V, const int64_t *offs, const int32_
             total += r.place(2);
         }
     }
-    return total;
+    if (over) *over = exceeded.load();
+    return exceeded.load() ? 0 : total;
 }
 
 uint64_t oracle_c4_rooted(int32_t V, const int64_t *offs, const int32_t *adj,

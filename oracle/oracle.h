@@ -89,6 +89,14 @@ uint64_t oracle_restricted_labelled(int32_t V, const int64_t *offs, const int32_
                                     int32_t nless, int32_t root_begin, int32_t root_end,
                                     int threads);
 
+/* As oracle_restricted_labelled, giving up (returning 0 with *over = 1)
+ * once about max_work candidates have been examined (max_work < 0: no cap). */
+uint64_t oracle_restricted_labelled_capped(int32_t V, const int64_t *offs,
+                                           const int32_t *adj, const char *pattern,
+                                           const int32_t *less, int32_t nless,
+                                           int32_t root_begin, int32_t root_end, int threads,
+                                           int64_t max_work, int *over);
+
 /* 4-cycles counted at a corner: for each v0 in [root_begin, root_end),
  * sum over x of C(c, 2), c = common neighbours v1 of v0 and x with v1 and x
  * above v0 (at_largest = 0: cycles whose smallest vertex is v0) or below it

@@ -44,6 +44,10 @@ def lib():
         l.oracle_restricted_labelled.restype = C.c_uint64
         l.oracle_restricted_labelled.argtypes = [C.c_int32, i64p, i32p, C.c_char_p, i32p,
                                                  C.c_int32, C.c_int32, C.c_int32, C.c_int]
+        l.oracle_restricted_labelled_capped.restype = C.c_uint64
+        l.oracle_restricted_labelled_capped.argtypes = [
+            C.c_int32, i64p, i32p, C.c_char_p, i32p, C.c_int32, C.c_int32, C.c_int32, C.c_int,
+            C.c_int64, C.POINTER(C.c_int)]
         l.oracle_c4_rooted.restype = C.c_uint64
         l.oracle_c4_rooted.argtypes = [C.c_int32, i64p, i32p, C.c_int32, C.c_int32, C.c_int,
                                        C.c_int]
@@ -144,6 +148,22 @@ def restricted_labelled(off, adj, pattern: str, less, roots=None, threads: int =
                                             len(less), b, e, threads)
 
 
+def restricted_labelled_capped(off, adj, pattern: str, less, roots, max_work: int,
+                               threads: int = 0):
+    """restricted_labelled, or None once about max_work candidates were
+    examined without finishing."""
+    V, o, a, po, pa = _csr(off, adj)
+    b, e = roots
+    flat = np.ascontiguousarray(np.array(less, np.int32).reshape(-1) if len(less)
+                                else np.zeros(2, np.int32))
+    over = C.c_int(0)
+    r = lib().oracle_restricted_labelled_capped(V, po, pa, pattern.encode(),
+                                                flat.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                len(less), b, e, threads, max_work,
+                                                C.byref(over))
+    return None if over.value else r
+
+
 def c4_rooted(off, adj, roots=None, at_largest: bool = False, threads: int = 0) -> int:
     """4-cycles whose smallest (at_largest: largest) vertex lies in roots."""
     V, o, a, po, pa = _csr(off, adj)
@@ -163,11 +183,12 @@ def degree_order(off, adj):
 
 
 def plan_conditions(dump: dict) -> tuple[str, list[tuple[int, int]]]:
-    """For an exact schedule dump: the pattern in the plan's vertex order
+    """For an exact schedule dump (or a pin record with the same "adj",
+    "perm" and "restrictions" fields): the pattern in the plan's vertex order
     (vertex i of the input becomes perm[i]) and its order conditions as
     pairs (a, b) meaning f(a) < f(b).  The dump's restriction (i, u) means
     the vertex at level u takes a smaller id than the one at level i."""
-    pat, perm = dump["pattern"], dump["perm"]
+    pat, perm = dump.get("pattern", dump.get("adj")), dump["perm"]
     n = len(perm)
     q = ["0"] * (n * n)
     for i in range(n):

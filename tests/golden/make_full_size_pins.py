@@ -21,7 +21,8 @@ graph (generated by libgat's seeded generators) and each pattern:
     vertex, the oracle's oracle_c4_rooted over the same ranges as well.
 
 Each range grows (x4) from one root until the oracle needs about --budget
-seconds on it.
+seconds on it; a root whose search alone is beyond that moves the range's
+start on (some hub roots of the 5- to 7-vertex patterns).
 
     python tests/golden/make_full_size_pins.py [--only c2,c3,...] [--budget 4]
 """
@@ -96,18 +97,30 @@ def csr_digest(off, adj) -> str:
     return h.hexdigest()
 
 
-def grow(fn, V: int, start: int, budget: float, max_width: int = 1 << 16):
+def grow(fn, V: int, start: int, budget: float, limit: int, max_width: int = 1 << 16):
     """[start, start + w) with w grown x4 from 1 while fn takes under
-    budget / 4 seconds; returns (begin, end, value, seconds)."""
-    w = 1
-    while True:
+    budget / 4 seconds; returns (begin, end, value, seconds), or None.  fn
+    returns None when it gives up (work cap): a wider range then keeps the
+    previous width, and a single root over the cap moves the start on by 1,
+    2, 4, ... roots, never to `limit` or beyond (the next range's start): hub
+    roots whose search alone exceeds the host budget are skipped."""
+    s0, step, w, best = start, 1, 1, None
+    while start < min(V, limit):
         e = min(V, start + w)
         t0 = time.time()
         val = fn(start, e)
         dt = time.time() - t0
+        if val is None:
+            if best is not None:
+                return best
+            start = s0 + step
+            step *= 2
+            continue
+        best = (start, e, int(val), dt)
         if dt >= budget / 4 or w >= max_width or e >= V:
-            return start, e, int(val), dt
+            return best
         w *= 4
+    return best
 
 
 def main() -> None:
@@ -141,17 +154,22 @@ def main() -> None:
             prec = {"adj": p, "perm": d["perm"], "restrictions": d["restrictions"],
                     "divisor": d["divisor"], "plan_ranges": []}
             secs = 0.0
-            for f in w["starts"]:
-                b, e, raw, dt = grow(lambda lo, hi: O.restricted_labelled(
-                    oo, oa, q, less, roots=(lo, hi), threads=a.threads), V, int(V * f),
-                    a.budget)
+            # about 1.5e8 candidates per second on 8 threads
+            cap = int(1.5e8 * a.budget * a.threads / 8)
+            starts = [int(V * f) for f in w["starts"]] + [V]
+            for s0, s1 in zip(starts, starts[1:]):
+                r = grow(lambda lo, hi: O.restricted_labelled_capped(
+                    oo, oa, q, less, (lo, hi), cap, threads=a.threads), V, s0, a.budget, s1)
+                if r is None:
+                    continue
+                b, e, raw, dt = r
                 prec["plan_ranges"].append([b, e, raw])
                 secs += dt
             if p == C4:
                 prec["c4_ranges"] = []
-                for f in w["starts"]:
+                for s0, s1 in zip(starts, starts[1:]):
                     b, e, c, dt = grow(lambda lo, hi: O.c4_rooted(
-                        oo, oa, roots=(lo, hi), threads=a.threads), V, int(V * f), a.budget)
+                        oo, oa, roots=(lo, hi), threads=a.threads), V, s0, a.budget, s1)
                     prec["c4_ranges"].append([b, e, c])
                     secs += dt
             prec["oracle_seconds"] = round(secs, 1)

@@ -249,38 +249,55 @@ def test_ref_mode_equals_reference_binary(gat, golden_graphs, golden_ref_engine,
             assert ex.count(g, s).count == e["ref_engine_answer"], (e["graph"], e["pattern"])
 
 
-def test_four_cycle_heavy_batches_and_row_scans(gat):
-    """The 4-cycle kernels' heavy path: a dense graph whose roots are all
-    heavy (degree >= 256), counted under a 1 MiB budget so the roots run in
-    many batches; a Barabasi-Albert graph whose few hub roots touch
-    thousands of counter lines; repeated calls (rows and line bitmaps must
-    come back zero) and shards.  All equal the schedule plan (checked
-    against the oracle on the smaller graphs of the other tests)."""
+def _bipartite_with_ring(gat, n: int):
+    """K_{2,n} (vertices 0 and 1 joined to 2 .. n+1) plus a ring through the
+    n leaves: vertices 0 and 1 share n >= 2^16 neighbours."""
+    import numpy as np
+
+    leaves = np.arange(2, n + 2, dtype=np.int64)
+    u = np.concatenate([np.zeros(n, np.int64), np.ones(n, np.int64), leaves])
+    v = np.concatenate([leaves, leaves, np.roll(leaves, -1)])
+    V = n + 2
+    key = np.unique(np.concatenate([u * V + v, v * V + u]))
+    off = np.zeros(V + 1, np.int64)
+    np.cumsum(np.bincount(key // V, minlength=V), out=off[1:])
+    return gat.Graph.from_csr(off, (key % V).astype(np.int32))
+
+
+def test_four_cycle_kernel_paths(gat, oracle):
+    """The 4-cycle kernels' paths: warp tables for light roots, roots
+    deferred to the CTA table, CTA windows over the ids (one window on a
+    dense graph, several when V exceeds a window), roots with more upper
+    neighbours than a CTA has threads, 32-bit window counters when a pair of
+    vertices shares 2^16 or more neighbours, odd V; repeated calls with one
+    executor across graphs, and shards.  Each count equals the host oracle's
+    count at each cycle's largest vertex and the schedule plan's."""
     c4 = "0101101001011010"
     s = gat.Schedule(c4, "exact")
     plan = _executor(gat, special_kernels=0)
-    cases = [(gat.Graph.erdos_renyi(600, 300.0, 11), 1 << 20),
-             (gat.Graph.barabasi_albert(20000, 8, 12), 16 << 20),
-             (gat.Graph.rmat(14, 1 << 17, 0.57, 0.19, 0.19, 13), 0),
-             (gat.Graph.barabasi_albert(3001, 8, 21), 256 << 20)]  # odd V: unaligned rows
-    wants = [plan.count(g, s).count for g, _ in cases]
-    # one executor across graphs whose scratch layouts differ, twice over
-    shared = _executor(gat, memory_budget=256 << 20)
+    cases = [gat.Graph.erdos_renyi(600, 300.0, 11),
+             gat.Graph.barabasi_albert(120000, 12, 12),
+             gat.Graph.rmat(14, 1 << 17, 0.57, 0.19, 0.19, 13),
+             gat.Graph.barabasi_albert(3001, 8, 21),
+             _bipartite_with_ring(gat, 70000)]
+    assert cases[1].info()[2] > 1024 and cases[4].info()[2] >= 1 << 16
+    wants = []
+    for g in cases:
+        off, adj = g.csr()
+        want = oracle.c4_rooted(off, adj, at_largest=True)
+        assert plan.count(g, s).count == want
+        wants.append(want)
+    assert wants[4] >= 70000 * 69999 // 2
+    shared = _executor(gat)
     for _ in range(2):
-        for (g, _), want in zip(cases, wants):
+        for g, want in zip(cases, wants):
             assert shared.count(g, s).count == want
-    for gi, (g, budget) in enumerate(cases):
-        want = plan.count(g, s).count
-        for tile, block in ((32, 256), (8, 128), (1, 64)):
-            ex = _executor(gat, threads_per_warp=tile, threads_per_block=block,
-                           memory_budget=budget)
-            for _ in range(2):
-                r = ex.count(g, s)
-                assert r.count == want, (gi, tile)
-            if gi < 2:
-                assert r.launches >= 3, r.launches  # heavy batches ran
-        ex = _executor(gat, memory_budget=budget)
-        assert sum(ex.count_shard(g, s, k, 5)[0] for k in range(5)) == want
+    for tile, block in ((32, 256), (8, 128)):
+        ex = _executor(gat, threads_per_warp=tile, threads_per_block=block)
+        for g, want in zip(cases, wants):
+            assert ex.count(g, s).count == want
+    for g, want in zip(cases, wants):
+        assert sum(shared.count_shard(g, s, k, 5)[0] for k in range(5)) == want
 
 
 def test_full_size_workload_graph_against_oracle(gat):

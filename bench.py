@@ -365,6 +365,60 @@ def oracle_port(off, adj, threads: int) -> dict:
                       "ranges of the degree-ordered graph: " + "; ".join(detail)}
 
 
+REF_CUDA_TIMEOUT_S = 75
+
+
+def reference_cuda(patterns: dict, counts: dict | None = None) -> dict:
+    """The reference's own CUDA engine on the same B200: target/pm.cu built
+    for sm_100a from the reference sources (oracle/Makefile target ref_gpu,
+    oracle/_ref/pm), run once per pattern on the workload graph file.  Its
+    `Time:` line covers Executor::perform_search with the graph resident
+    (target/pm.cu:56-64), the same region as this engine's device time; its
+    `Answer:` is the reference engine's own number, not the exact count
+    (restrictions outside the basic vertices are dropped, and per-level int
+    counters overflow on large graphs).  Reported once, outside the steps."""
+    import re
+
+    binary = ROOT / "oracle/_ref/pm"
+    if not binary.exists():
+        return {"unavailable": "oracle/_ref/pm not built (make -C oracle ref_gpu)"}
+    out = {"binary": "oracle/_ref/pm (target/pm.cu, sm_100a, default generated config)"}
+    for name, p in patterns.items():
+        try:
+            r = subprocess.run([str(binary), str(graph_cache_path()), p], capture_output=True,
+                               text=True, timeout=REF_CUDA_TIMEOUT_S)
+        except subprocess.TimeoutExpired:
+            out[name] = {"finished": False,
+                         "note": f"no answer within {REF_CUDA_TIMEOUT_S} s (process stopped)"}
+            continue
+        ans = re.search(r"Answer: (-?\d+)", r.stdout)
+        tm = re.search(r"Time: (\d+) us", r.stdout)
+        rec = {"finished": r.returncode == 0 and tm is not None, "rc": r.returncode,
+               "answer": int(ans.group(1)) if ans else None,
+               "seconds": int(tm.group(1)) / 1e6 if tm else None}
+        if rec["seconds"] and counts and name in counts:
+            rec["exact_matches_per_s"] = counts[name] / rec["seconds"]
+        if not rec["finished"]:
+            rec["tail"] = (r.stdout + r.stderr)[-300:]
+        out[name] = rec
+    return out
+
+
+def exact_counts() -> dict | None:
+    """The workload's exact counts as pinned by the oracle
+    (tests/golden/c2_oracle.json), for rates of engines that do not return
+    them."""
+    p = ROOT / "tests/golden/c2_oracle.json"
+    try:
+        d = json.loads(p.read_text())
+        # the oracle's restatement of the reference engine counts each
+        # 4-clique 4 times; the 4-cycle total is the whole-graph count
+        return {"k4": int(d["k4"]["ref_engine_oracle"]) // 4,
+                "c4": int(d["c4"]["exact_at_largest_vertex"])}
+    except Exception:
+        return None
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -378,7 +432,7 @@ def run_reference(args):
     maxdeg = int((off[1:] - off[:-1]).max())
     auts = [pyoracle.automorphisms(p) for p in PATTERNS.values()]
     # each step about 150 / (steps + warmup) s, so the whole run takes minutes
-    budget = max(1.0, min(15.0, 150.0 / max(1, args.steps + args.warmup)))
+    budget = max(1.0, min(12.0, 100.0 / max(1, args.steps + args.warmup)))
     plans = naive_plans(off, adj, budget, threads)
     for _ in range(args.warmup):
         [run_naive(pl, threads) for pl in plans]
@@ -400,6 +454,7 @@ def run_reference(args):
                          "estimated_workload_seconds": est["estimated_workload_seconds"]},
         "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference_cuda": reference_cuda(PATTERNS, exact_counts()),
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -220,15 +220,22 @@ class Graph(_Handle):
 
     @classmethod
     def rmat(cls, scale: int, samples: int, a: float = 0.57, b: float = 0.19,
-             c: float = 0.19, seed: int = 0) -> "Graph":
-        g = cls()
-        check(lib().gat_graph_generate(1, scale, samples, a, b, c, seed, C.byref(g._h)))
-        return g
+             c: float = 0.19, seed: int = 0, device: bool = False) -> "Graph":
+        """Seeded R-MAT graph; device=True draws and builds it on the current
+        GPU (identical result, resident there afterwards)."""
+        return cls._generate(1, (scale, samples, a, b, c), seed, device)
 
     @classmethod
-    def barabasi_albert(cls, n: int, m: int, seed: int) -> "Graph":
+    def barabasi_albert(cls, n: int, m: int, seed: int, device: bool = False) -> "Graph":
+        return cls._generate(2, (n, m, 0, 0, 0), seed, device)
+
+    @classmethod
+    def _generate(cls, kind: int, p: tuple, seed: int, device: bool) -> "Graph":
         g = cls()
-        check(lib().gat_graph_generate(2, n, m, 0, 0, 0, seed, C.byref(g._h)))
+        if device:
+            check(lib().gat_graph_generate_device(kind, *p, seed, None, C.byref(g._h)))
+        else:
+            check(lib().gat_graph_generate(kind, *p, seed, C.byref(g._h)))
         return g
 
     def save(self, path: str) -> None:

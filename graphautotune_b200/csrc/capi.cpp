@@ -58,6 +58,7 @@ struct DevCopy {
     int64_t *lo_off = nullptr;
     int64_t lo_total = 0;
     int32_t max_degree = 0;
+    int32_t max_lower = 0;  // longest lower list (entries below the row's vertex)
     bool ready = false;
     std::vector<int64_t> lo_host;   // host copy of lo_off
     std::vector<int64_t> off_host;  // host copy of off
@@ -83,6 +84,7 @@ struct DevCopy {
         lo_off = nullptr;
         lo_total = 0;
         max_degree = 0;
+        max_lower = 0;
         ready = false;
         lo_host.clear();
         off_host.clear();
@@ -510,6 +512,12 @@ int gat_graph_csr(const gat_graph *g, const int64_t **offsets, const int32_t **a
 }
 
 namespace {
+// Device rows are allocated 4 ints longer than the edge list: kernels that
+// read aligned 16-byte groups (cliques.cu) may touch up to 3 entries past
+// the last row.
+constexpr int64_t kAdjPadInts = 4;
+int64_t adj_alloc_ints(int64_t E) { return E + kAdjPadInts; }
+
 // Completes a device copy whose off and adj are in place: lo_off is derived
 // on the device, and both offset arrays are kept on the host too (range and
 // shard arithmetic reads them).  `off_known` is the host's copy of off when
@@ -538,6 +546,9 @@ int finish_copy(DevCopy &d, int32_t V, int32_t max_degree, const std::vector<int
     }
     d.lo_total = d.lo_host[size_t(V)];
     d.max_degree = max_degree;
+    int64_t ml = 0;
+    for (size_t v = 0; v < size_t(V); v++) ml = std::max(ml, d.lo_host[v + 1] - d.lo_host[v]);
+    d.max_lower = (int32_t)ml;
     d.ready = true;
     return GAT_OK;
 }
@@ -546,7 +557,7 @@ int upload_copy(const HostGraph &h, DevCopy &d, cudaStream_t st) {
     d.release();
     cudaError_t e;
     if ((e = cudaMalloc(&d.off, sizeof(int64_t) * (h.V + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&d.adj, sizeof(int32_t) * std::max<int64_t>(h.E, 1))) != cudaSuccess) {
+        (e = cudaMalloc(&d.adj, sizeof(int32_t) * adj_alloc_ints(h.E))) != cudaSuccess) {
         d.release();
         return fail(GAT_ERR_MEMORY, std::string("device graph allocation: ") + cudaGetErrorString(e));
     }
@@ -572,7 +583,7 @@ int derive_ordered_copy(const HostGraph &h, const DevCopy &src, DevCopy &d, cuda
     d.release();
     cudaError_t e;
     if ((e = cudaMalloc(&d.off, sizeof(int64_t) * (h.V + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&d.adj, sizeof(int32_t) * std::max<int64_t>(h.E, 1))) != cudaSuccess) {
+        (e = cudaMalloc(&d.adj, sizeof(int32_t) * adj_alloc_ints(h.E))) != cudaSuccess) {
         d.release();
         return fail(GAT_ERR_MEMORY, std::string("device graph allocation: ") + cudaGetErrorString(e));
     }
@@ -587,6 +598,17 @@ int derive_ordered_copy(const HostGraph &h, const DevCopy &src, DevCopy &d, cuda
 
 // Hub bitmaps for the vertices of degree >= min_degree, largest degree first,
 // as many as fit in max_bytes.
+void release_hubs(DevCopy &d) {
+    cudaFree(d.hub_slot);
+    cudaFree(d.hubs);
+    cudaFree(d.bitmaps);
+    d.hub_slot = nullptr;
+    d.hubs = nullptr;
+    d.bitmaps = nullptr;
+    d.nhubs = 0;
+    d.bitmap_words = 0;
+}
+
 int upload_hubs(DevCopy &d, int32_t V, int64_t min_degree, int64_t max_bytes,
                 cudaStream_t st) {
     if (min_degree <= 0 || max_bytes <= 0 || V == 0) return GAT_OK;
@@ -624,6 +646,78 @@ int upload_hubs(DevCopy &d, int32_t V, int64_t min_degree, int64_t max_bytes,
 }
 }  // namespace
 
+int gat_graph_generate_device(int kind, double p0, double p1, double p2, double p3, double p4,
+                              uint64_t seed, void *stream, gat_graph **out) {
+    if (!out) return fail(GAT_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    cudaStream_t st = (cudaStream_t)stream;
+    auto g = std::make_unique<gat_graph>();
+    DevCopy &d = g->dev;
+    int32_t V = 0;
+    int64_t E = 0;
+    cudaError_t e = cudaSuccess;
+    std::vector<std::pair<int32_t, int32_t>> edges;
+    if (kind == 1) {
+        if (p0 < 1 || p0 > 30 || p1 < 0 || p2 < 0 || p3 < 0 || p4 < 0 || p2 + p3 + p4 > 1)
+            return fail(GAT_ERR_ARGUMENT, "bad R-MAT parameters");
+        V = int32_t(1) << (int)p0;
+    } else if (kind == 0) {
+        if (p0 < 0 || p0 > INT32_MAX || p1 < 0) return fail(GAT_ERR_ARGUMENT, "bad ER parameters");
+        V = (int32_t)p0;
+        gen_erdos_renyi_edges(V, p1, seed, edges);
+    } else if (kind == 2) {
+        if (p0 < 0 || p0 > INT32_MAX || p1 < 1) return fail(GAT_ERR_ARGUMENT, "bad BA parameters");
+        V = (int32_t)p0;
+        gen_barabasi_albert_edges(V, (int32_t)p1, seed, edges);
+    } else {
+        return fail(GAT_ERR_ARGUMENT, "unknown generator");
+    }
+    if ((e = cudaMalloc(&d.off, sizeof(int64_t) * (size_t(V) + 1))) != cudaSuccess) {
+        d.release();
+        return fail(GAT_ERR_MEMORY, std::string("device graph allocation: ") + cudaGetErrorString(e));
+    }
+    if (kind == 1) {
+        e = rmat_csr_device((int)p0, (int64_t)p1, p2, p3, p4, seed, d.off, &d.adj,
+                            kAdjPadInts, &E, st);
+    } else {
+        int32_t *pairs = nullptr;
+        const size_t bytes = sizeof(int32_t) * 2 * std::max<size_t>(edges.size(), 1);
+        if ((e = cudaMalloc(&pairs, bytes)) == cudaSuccess &&
+            (edges.empty() ||
+             (e = cudaMemcpyAsync(pairs, edges.data(), sizeof(int32_t) * 2 * edges.size(),
+                                  cudaMemcpyHostToDevice, st)) == cudaSuccess))
+            e = pairs_csr_device(pairs, (int64_t)edges.size(), V, d.off, &d.adj,
+                                 kAdjPadInts, &E, st);
+        const cudaError_t f = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) e = f;
+        cudaFree(pairs);
+    }
+    if (e != cudaSuccess) {
+        d.release();
+        return cuda_fail(e, "device graph build");
+    }
+    HostGraph &h = g->host;
+    h.V = V;
+    h.E = E;
+    h.off.resize(size_t(V) + 1);
+    h.adj.resize(size_t(E));
+    if ((e = cudaMemcpyAsync(h.off.data(), d.off, sizeof(int64_t) * (size_t(V) + 1),
+                             cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (E > 0 && (e = cudaMemcpyAsync(h.adj.data(), d.adj, sizeof(int32_t) * size_t(E),
+                                       cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        d.release();
+        return cuda_fail(e, "device graph read-back");
+    }
+    int rc = finish_copy(d, V, h.max_degree(), &h.off, st);
+    if (rc != GAT_OK) return rc;
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    g->device = dev;
+    *out = g.release();
+    return GAT_OK;
+}
+
 int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
                         int64_t hub_max_bytes, void *stream) {
     if (!g) return fail(GAT_ERR_ARGUMENT, "null argument");
@@ -632,11 +726,23 @@ int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     const int32_t V = g->host.V;
-    int rc = upload_copy(g->host, g->dev, st);
+    // A graph's host CSR never changes, so a copy already resident on this
+    // device (built there by gat_graph_generate_device, or uploaded before)
+    // is kept; its hub bitmaps are rebuilt for the requested parameters.
+    int rc = GAT_OK;
+    if (g->dev.ready && g->device == dev)
+        release_hubs(g->dev);
+    else
+        rc = upload_copy(g->host, g->dev, st);
     if (rc == GAT_OK) rc = upload_hubs(g->dev, V, hub_min_degree, hub_max_bytes, st);
     if (rc != GAT_OK) return rc;
     if (flags & GAT_UPLOAD_DEGREE_ORDER) {
-        rc = derive_ordered_copy(g->host, g->dev, g->dev_ordered, st);
+        if (g->dev_ordered.ready && g->device == dev) {
+            release_hubs(g->dev_ordered);
+            rc = GAT_OK;
+        } else {
+            rc = derive_ordered_copy(g->host, g->dev, g->dev_ordered, st);
+        }
         if (rc == GAT_OK)
             rc = upload_hubs(g->dev_ordered, V, hub_min_degree, hub_max_bytes, st);
         if (rc != GAT_OK) return rc;
@@ -792,6 +898,82 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
     return GAT_OK;
 }
 
+// The exact k-clique count through the bit-matrix kernels (cliques.cu) over
+// roots [vb, ve).  Scratch: the root cursors, and per-CTA matrix rows only
+// when the graph's longest lower list does not fit in shared memory.
+int run_clique(gat_executor *e, const DevGraphView &view, int k, int64_t vb, int64_t ve,
+               cudaStream_t strm, bool balg, uint64_t *count, gat_stats *stats,
+               std::chrono::steady_clock::time_point t0) {
+    int wocc = 0, cocc = 0;
+    clique_blocks_per_sm(k, balg, &wocc, &cocc);
+    if (wocc <= 0 || cocc <= 0) return fail(GAT_ERR_CUDA, "clique kernels do not fit on the device");
+    const int warp_grid = e->sms * wocc;
+    const int cta_grid = e->cfg.num_blocks > 0 ? std::min(e->cfg.num_blocks, e->sms * cocc)
+                                               : e->sms * cocc;
+    auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
+    const int64_t aux_bytes = al(sizeof(CliqueAux));
+    const int64_t stride = clique_rows_words(view.max_lower);
+    const int64_t rows_bytes = al(int64_t(cta_grid) * stride * 4);
+    const size_t need = size_t(aux_bytes + rows_bytes);
+    cudaError_t ce;
+    if (need > e->scratch_bytes) {
+        cudaFree(e->scratch);
+        e->scratch = nullptr;
+        e->scratch_bytes = 0;
+        if ((ce = cudaMalloc(&e->scratch, need)) != cudaSuccess)
+            return fail(GAT_ERR_MEMORY, std::string("clique scratch: ") + cudaGetErrorString(ce));
+        e->scratch_bytes = need;
+    }
+    e->scratch_clean = false;
+    unsigned char *base = reinterpret_cast<unsigned char *>(e->scratch);
+    CliqueLaunch L;
+    L.g = view;
+    L.k = k;
+    L.v_begin = vb;
+    L.v_end = ve;
+    L.warp_grid = warp_grid;
+    L.cta_grid = cta_grid;
+    L.ctr = e->ctr;
+    L.aux = reinterpret_cast<CliqueAux *>(base);
+    L.rows = stride > 0 ? reinterpret_cast<uint32_t *>(base + aux_bytes) : nullptr;
+    L.rows_stride = stride;
+    L.stats = balg;
+    cudaEventRecord(e->ev0, strm);
+    ce = launch_clique(L, strm);
+    if (ce != cudaSuccess) return cuda_fail(ce, "clique launch");
+    cudaEventRecord(e->ev1, strm);
+    if ((ce = cudaMemcpyAsync(e->host_ctr, e->ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost,
+                              strm)) != cudaSuccess ||
+        (ce = cudaStreamSynchronize(strm)) != cudaSuccess)
+        return cuda_fail(ce, "clique count");
+    if (e->host_ctr->error) return fail(GAT_ERR_DEVICE, "clique kernel reported an internal error");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    const int64_t raw = (int64_t)e->host_ctr->result;
+    *count = (uint64_t)raw;
+    gat_stats st{};
+    st.kernel_ms = ms;
+    st.raw_sum = raw;
+    st.divisor = 1;
+    st.tasks = (uint64_t)(ve - vb);
+    st.balg_bytes = e->host_ctr->bytes;
+    st.grid = cta_grid;
+    st.block = 256;
+    st.tile = 32;
+    st.launches = ve > vb ? 2 : 0;
+    st.scratch_bytes = (int64_t)need;
+    st.total_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) *stats = st;
+    return GAT_OK;
+}
+
+// First vertex v whose units start at or after unit u, units numbered by
+// the prefix sums `units` (V + 1 entries).
+int64_t first_root_at(const std::vector<int64_t> &units, int64_t u) {
+    return std::lower_bound(units.begin(), units.end() - 1, u) - units.begin();
+}
+
 int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *stream,
                uint64_t *count, gat_stats *stats, bool balg, int64_t root_begin = -1,
                int64_t root_end = -1, int shard = 0, int num_shards = 0) {
@@ -833,6 +1015,7 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
     view.lo_off = dc->lo_off;
     view.lo_total = dc->lo_total;
     view.max_degree = dc->max_degree;
+    view.max_lower = dc->max_lower;
     view.hub_slot = dc->hub_slot;
     view.bitmaps = dc->bitmaps;
     view.bitmap_words = dc->bitmap_words;
@@ -862,8 +1045,24 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
         shape.task_begin = toff[root_begin];
         shape.task_end = toff[root_end];
     }
+    if (plan.special == GAT_SPECIAL_CLIQUE && s->mode == GAT_MODE_EXACT &&
+        e->cfg.special_kernels == 1 && view.lo_off != nullptr &&
+        view.max_lower <= kCliqueMaxLower) {
+        // Largest-vertex range of this call: whole graph, a root range, or
+        // the roots whose level-1 units (lower neighbours) start in the
+        // shard's unit range.
+        int64_t vb = 0, ve = view.V;
+        if (root_begin >= 0) {
+            vb = root_begin;
+            ve = root_end;
+        } else if (num_shards > 0) {
+            vb = first_root_at(dc->lo_host, shape.task_begin);
+            ve = shard + 1 == num_shards ? view.V : first_root_at(dc->lo_host, shape.task_end);
+        }
+        return run_clique(e, view, plan.n, vb, ve, strm, balg, count, stats, t0);
+    }
     if (plan.special == GAT_SPECIAL_C4 && s->mode == GAT_MODE_EXACT &&
-        e->cfg.special_kernels != 0) {
+        e->cfg.special_kernels == 1) {
         // First-vertex range of this call: whole graph, a root range, or the
         // vertices whose level-1 units start inside the shard's unit range.
         int64_t vb = 0, ve = view.V;

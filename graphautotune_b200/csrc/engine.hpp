@@ -20,6 +20,7 @@ struct DevGraphView {
     const int64_t *lo_off = nullptr;
     int64_t lo_total = 0;  // lo_off[V]
     int32_t max_degree = 0;
+    int32_t max_lower = 0;  // max over v of lo_off[v + 1] - lo_off[v]
     // Hub bitmaps: bit x of row hub_slot[v] is set iff x is in N(v), for
     // the vertices with hub_slot[v] >= 0 (null when none were built).
     const int32_t *hub_slot = nullptr;
@@ -90,6 +91,45 @@ int c4_light_blocks_per_sm(bool stats);
 int c4_root_blocks_per_sm(bool wide, bool stats);
 cudaError_t launch_c4(const C4Launch &launch, cudaStream_t st);
 
+// Exact k-clique count (4 <= k <= 7) over largest-id vertices [v_begin, v_end)
+// (plans with special == GAT_SPECIAL_CLIQUE) by bit-matrix induced subgraphs
+// of each root's lower list (cliques.cu).  Needs lo_off, every lower list of
+// at most kCliqueMaxLower entries, and adj readable 4 ints past its end.
+// `rows` holds cta_grid slices of rows_stride words when
+// clique_rows_words(max lower degree) > 0, else it may be null.
+constexpr int kCliqueMaxLower = 2048;
+struct CliqueAux {
+    unsigned long long warp_cursor;
+    unsigned long long cta_cursor;
+    unsigned long long pad[2];
+};
+struct CliqueLaunch {
+    DevGraphView g;
+    int k = 4;
+    int64_t v_begin = 0, v_end = 0;
+    int warp_grid = 0, cta_grid = 0;
+    DevCounters *ctr = nullptr;
+    CliqueAux *aux = nullptr;
+    uint32_t *rows = nullptr;
+    int64_t rows_stride = 0;
+    bool stats = false;
+};
+int64_t clique_rows_words(int32_t max_lower);
+void clique_blocks_per_sm(int k, bool stats, int *warp_occ, int *cta_occ);
+cudaError_t launch_clique(const CliqueLaunch &launch, cudaStream_t st);
+
+// Graph construction on the device (gen.cu).  Both write off[V + 1] (caller
+// allocated) and allocate *adj with pad_ints ints past the E entries; E is
+// the number of directed entries of the symmetric, loop-free, deduplicated
+// CSR with sorted rows.
+// R-MAT exactly as graph.cpp gen_rmat + build_csr compute it.
+cudaError_t rmat_csr_device(int scale, int64_t samples, double a, double b, double c,
+                            uint64_t seed, int64_t *off, int32_t **adj, int64_t pad_ints,
+                            int64_t *E, cudaStream_t st);
+// An undirected edge list of n (u, v) pairs (device memory) on V vertices.
+cudaError_t pairs_csr_device(const int32_t *pairs, int64_t n, int32_t V, int64_t *off,
+                             int32_t **adj, int64_t pad_ints, int64_t *E, cudaStream_t st);
+
 // Batched launches: host code fills an array of batch_job_bytes()-sized job
 // records (one per (plan, graph) pair), copies it and the chunk-aligned
 // virtual start of every job to the device, and launches one persistent
@@ -118,6 +158,7 @@ int count_noalloc(const GatPlan &plan, const int64_t *d_off, const int32_t *d_ad
 enum : unsigned long long {
     GAT_DEVERR_SCRATCH = 1ull,  // a stored set would overflow its slot
     GAT_DEVERR_TABLE = 2ull,    // a shared-memory count table ran out of slots
+    GAT_DEVERR_WAIT = 4ull,     // a bulk copy did not complete within the wait bound
 };
 
 // Shared memory one tile needs.

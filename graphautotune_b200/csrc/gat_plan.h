@@ -23,6 +23,7 @@
 #define GAT_MAX_TERMS 64
 
 #define GAT_SPECIAL_C4 1
+#define GAT_SPECIAL_CLIQUE 2
 
 enum {
     GAT_SET_ALIAS = 0,  /* N(v_level), truncated by p_trunc */
@@ -42,9 +43,10 @@ typedef struct GatPlan {
     int32_t num_store;     /* materialised prefixes = scratch slots per tile */
     int32_t iep_num;       /* IEP value slots */
     int32_t num_terms;     /* IEP subgroups */
-    int32_t special;       /* 0: interpret this plan; GAT_SPECIAL_C4: the
-                              exact 4-cycle count has a dedicated kernel
-                              (the plan stays valid as its fallback) */
+    int32_t special;       /* 0: interpret this plan; GAT_SPECIAL_C4 /
+                              GAT_SPECIAL_CLIQUE: the exact 4-cycle or
+                              k-clique count has a dedicated kernel (the
+                              plan stays valid as its fallback) */
     int64_t divisor;       /* final count = sum / divisor */
     int32_t lane_last;     /* 1: every prefix of level basic-1 is COUNT and
                               every IEP slot is one of them (<= 8 slots), so

@@ -197,6 +197,13 @@ uint64_t stream_state(uint64_t seed, uint64_t i) {
 
 void gen_erdos_renyi(int32_t n, double avg_degree, uint64_t seed, HostGraph &g) {
     std::vector<std::pair<int32_t, int32_t>> edges;
+    gen_erdos_renyi_edges(n, avg_degree, seed, edges);
+    build_csr(n, edges, g);
+}
+
+void gen_erdos_renyi_edges(int32_t n, double avg_degree, uint64_t seed,
+                           std::vector<std::pair<int32_t, int32_t>> &edges) {
+    edges.clear();
     double p = n > 1 ? avg_degree / double(n - 1) : 0.0;
     if (p > 0 && p < 1) {
         uint64_t s = stream_state(seed, 0);
@@ -215,7 +222,6 @@ void gen_erdos_renyi(int32_t n, double avg_degree, uint64_t seed, HostGraph &g) 
         for (int32_t v = 1; v < n; v++)
             for (int32_t w = 0; w < v; w++) edges.emplace_back(v, w);
     }
-    build_csr(n, edges, g);
 }
 
 void gen_rmat(int scale, int64_t samples, double a, double b, double c,
@@ -243,10 +249,14 @@ void gen_rmat(int scale, int64_t samples, double a, double b, double c,
 
 void gen_barabasi_albert(int32_t n, int32_t m, uint64_t seed, HostGraph &g) {
     std::vector<std::pair<int32_t, int32_t>> edges;
-    if (m < 1 || n <= m) {
-        build_csr(std::max(n, 0), edges, g);
-        return;
-    }
+    gen_barabasi_albert_edges(n, m, seed, edges);
+    build_csr(std::max(n, 0), edges, g);
+}
+
+void gen_barabasi_albert_edges(int32_t n, int32_t m, uint64_t seed,
+                               std::vector<std::pair<int32_t, int32_t>> &edges) {
+    edges.clear();
+    if (m < 1 || n <= m) return;
     uint64_t s = stream_state(seed, 0);
     // `ends` holds every edge endpoint, so a uniform pick from it is a pick
     // proportional to degree.
@@ -272,7 +282,6 @@ void gen_barabasi_albert(int32_t n, int32_t m, uint64_t seed, HostGraph &g) {
             ends.push_back(t);
         }
     }
-    build_csr(n, edges, g);
 }
 
 void relabel_by_degree(const HostGraph &in, HostGraph &out,

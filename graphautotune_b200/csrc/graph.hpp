@@ -51,6 +51,11 @@ void gen_rmat(int scale, int64_t samples, double a, double b, double c,
 // each new vertex joins m distinct existing vertices drawn in proportion to
 // degree.
 void gen_barabasi_albert(int32_t n, int32_t m, uint64_t seed, HostGraph &g);
+// The undirected edge lists those two generators pass to build_csr.
+void gen_erdos_renyi_edges(int32_t n, double avg_degree, uint64_t seed,
+                           std::vector<std::pair<int32_t, int32_t>> &edges);
+void gen_barabasi_albert_edges(int32_t n, int32_t m, uint64_t seed,
+                               std::vector<std::pair<int32_t, int32_t>> &edges);
 
 // Relabels vertices by decreasing degree (ties: increasing old id); new id 0
 // is the largest hub.  `new_of_old` receives the map.

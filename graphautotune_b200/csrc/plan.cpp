@@ -412,6 +412,16 @@ bool build_exact_plan(const Pattern &p, const ExactCand &best, int64_t aut, Plan
         for (int i = 0; i < 4; i++) cyc &= __builtin_popcount(p.row[i]) == 2;
         if (cyc) pl.special = GAT_SPECIAL_C4;
     }
+    // Complete patterns on 4..7 vertices have the bit-matrix clique kernels
+    // when the plan roots each clique at its largest vertex: every enumerated
+    // level below all earlier ones and divisor 1 (so the counted vertex is
+    // the smallest).
+    if (p.n >= 4 && p.n <= 7 && p.edges() == p.n * (p.n - 1) / 2 && pl.divisor == 1 &&
+        pl.level1_bounded) {
+        bool chain = true;
+        for (int k = 1; k < pl.basic; k++) chain &= pl.l_bound[k] == (1u << k) - 1u;
+        if (chain) pl.special = GAT_SPECIAL_CLIQUE;
+    }
     return true;
 }
 }  // namespace

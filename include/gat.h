@@ -131,11 +131,15 @@ typedef struct gat_config {
                                       take units one each) */
     int32_t hub_bitmaps;           /* 1: intersect against the graph's hub
                                       bitmaps where cheaper; 0: never */
-    int64_t memory_budget;         /* bytes of scratch the executor may hold;
-                                      0 = 4 GiB (16 GiB for the 4-cycle
-                                      kernel's counter rows) */
+    int64_t memory_budget;         /* bytes of set scratch the executor may
+                                      hold for the schedule-plan search;
+                                      0 = 4 GiB */
     int32_t special_kernels;       /* 1: patterns with a dedicated kernel use
-                                      it (exact 4-cycle); 0: always the plan */
+                                      it (exact 4-cycle, exact 4- to
+                                      7-cliques) and plans use the
+                                      lane-per-candidate last level; 2: the
+                                      lane path but no dedicated kernel;
+                                      0: the plan interpreter alone */
     int32_t reserved1;
     int64_t reserved[3];
 } gat_config;
@@ -172,6 +176,17 @@ int gat_graph_validate(const gat_graph *g, int check_symmetry);
  * p2..p4 = a, b, c), 2 Barabasi-Albert (p0 = n, p1 = m). */
 int gat_graph_generate(int kind, double p0, double p1, double p2, double p3,
                        double p4, uint64_t seed, gat_graph **out);
+/* The same seeded graphs built on the current device: R-MAT edges are drawn
+ * there (the same splitmix64 streams, so the graph is identical to
+ * gat_graph_generate's), Erdos-Renyi and Barabasi-Albert edge lists are drawn
+ * on the host; symmetrising, dropping self loops and duplicates and sorting
+ * the rows run on the device, and the CSR is copied back for the host view.
+ * The device copy stays resident (gat_graph_upload then only adds the
+ * degree-ordered copy and hub bitmaps).  Replaces the reference's host-side
+ * graph construction (infra/graph_backend.cuh:23-89) and
+ * utils/graph_transform.cu:6-28 for synthetic inputs. */
+int gat_graph_generate_device(int kind, double p0, double p1, double p2, double p3,
+                              double p4, uint64_t seed, void *stream, gat_graph **out);
 int gat_graph_save(const gat_graph *g, const char *path);
 int gat_graph_info(const gat_graph *g, int32_t *V, int64_t *E,
                    int32_t *max_degree);

@@ -204,17 +204,17 @@ def test_relabelling_and_sharding_invariance(gat, executors):
 
 
 def test_lane_last_level_equals_tile_path(gat, oracle, golden_schedules):
-    """The one-candidate-per-lane last level (special_kernels=1) gives the
-    same counts and the same algorithmic byte totals as the tile-cooperative
-    path (special_kernels=0), on every tile width, with and without hub
-    bitmaps, in both modes."""
+    """The one-candidate-per-lane last level (special_kernels=2: the lane
+    path without the dedicated 4-cycle and clique kernels) gives the same
+    counts and the same algorithmic byte totals as the tile-cooperative path
+    (special_kernels=0), on every tile width, with and without hub bitmaps,
+    in both modes."""
     shapes = ((32, 256, 8), (8, 128, 1), (1, 128, 16))
-    lanes = [_executor(gat, threads_per_warp=t, threads_per_block=b, chunk=c)
-             for t, b, c in shapes]
+    lanes = [_executor(gat, threads_per_warp=t, threads_per_block=b, chunk=c,
+                       special_kernels=2) for t, b, c in shapes]
     tiles = [_executor(gat, threads_per_warp=t, threads_per_block=b, chunk=c,
                        special_kernels=0) for t, b, c in shapes]
-    pats = [p for p in NAMED + gat.enumerate_patterns(5)
-            if p != "0101101001011010"]  # the 4-cycle has its own kernel
+    pats = NAMED + gat.enumerate_patterns(5)
     graphs = [_graph(gat, *m) for m in MEDIUM]
     hubby = gat.Graph.rmat(12, 1 << 15, 0.57, 0.19, 0.19, 9)
     hubby.upload(degree_order=True, hub_min_degree=8, hub_max_bytes=1 << 28)

@@ -56,3 +56,40 @@ def test_counts_on_device_relabelled_copy(gat, oracle):
     for _ in range(2):
         g.upload(degree_order=True)
         assert [ex.count(g, gat.Schedule(p, "exact")).count for p in pats] == want
+
+
+def test_device_generated_graphs_equal_host_generated(gat):
+    """gat_graph_generate_device: R-MAT drawn on the GPU, and Erdos-Renyi /
+    Barabasi-Albert edge lists deduplicated into CSR on the GPU, give the
+    host generators' graphs entry for entry (self loops and duplicate samples
+    included in the R-MAT draws), and the resident copy counts like an
+    uploaded one."""
+    cases = [
+        ("rmat", (12, 1 << 15, 0.57, 0.19, 0.19, 9)),
+        ("rmat", (16, 1 << 20, 0.57, 0.19, 0.19, 2)),
+        ("rmat", (3, 100, 0.45, 0.15, 0.15, 1)),   # dense: many duplicates and loops
+        ("ba", (3000, 7, 4)),
+        ("er", (5000, 0.7, 3)),
+    ]
+    for kind, p in cases:
+        if kind == "rmat":
+            h, d = gat.Graph.rmat(*p), gat.Graph.rmat(*p, device=True)
+        elif kind == "ba":
+            h, d = gat.Graph.barabasi_albert(*p), gat.Graph.barabasi_albert(*p, device=True)
+        else:
+            h = gat.Graph.erdos_renyi(*p)
+            d = gat.Graph._generate(0, (p[0], p[1], 0, 0, 0), p[2], True)
+        assert h.info() == d.info(), (kind, p)
+        ho, ha = h.csr()
+        do, da = d.csr()
+        assert np.array_equal(ho, do) and np.array_equal(ha, da), (kind, p)
+        d.upload(degree_order=True)
+        go, ga = d.ordered_csr()
+        want_off, want_adj = host_relabel(ho, ha)
+        assert np.array_equal(go, want_off) and np.array_equal(ga, want_adj), (kind, p)
+    g = gat.Graph.rmat(13, 1 << 17, 0.57, 0.19, 0.19, 5, device=True)
+    ex = gat.Executor()
+    for pat in ("011101110", "0111101111011110", "0101101001011010"):
+        s = gat.Schedule(pat, "exact")
+        assert ex.count(g, s).count == ex.count(gat.Graph.rmat(13, 1 << 17, 0.57, 0.19, 0.19, 5),
+                                                s).count

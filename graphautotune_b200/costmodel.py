@@ -301,6 +301,28 @@ def pick(model: CostModel, gf: np.ndarray, pf: np.ndarray, points: list[dict]) -
     return points[int(np.argmin(model.predict(X)))]
 
 
+# The model leaves the default configuration only for a predicted gain of at
+# least this factor: its ranking error on held-out graphs is of that order.
+MIN_PREDICTED_GAIN = 1.15
+
+
+def choose(model: CostModel, gf: np.ndarray, pf: np.ndarray, points: list[dict],
+           default: dict, min_gain: float = MIN_PREDICTED_GAIN) -> tuple[dict, bool]:
+    """The model's choice among `points`, falling back to `default` unless
+    the best prediction beats the default's by min_gain.  Returns (point,
+    whether the default was kept)."""
+    cand = list(points)
+    if all(tuner.fingerprint(d) != tuner.fingerprint(default) for d in cand):
+        cand.append(default)
+    X = np.stack([features(gf, pf, d) for d in cand])
+    pred = model.predict(X)
+    di = [tuner.fingerprint(d) for d in cand].index(tuner.fingerprint(default))
+    bi = int(np.argmin(pred))
+    if pred[bi] + math.log(min_gain) <= pred[di]:
+        return cand[bi], False
+    return default, True
+
+
 # ---------------------------------------------------------------- CLI
 
 def main():

@@ -901,9 +901,13 @@ int run_c4(gat_executor *e, const DevGraphView &view, const DevCopy &dc, int64_t
 // The exact k-clique count through the bit-matrix kernels (cliques.cu) over
 // roots [vb, ve).  Scratch: the root cursors, and per-CTA matrix rows only
 // when the graph's longest lower list does not fit in shared memory.
-int run_clique(gat_executor *e, const DevGraphView &view, int k, int64_t vb, int64_t ve,
-               cudaStream_t strm, bool balg, uint64_t *count, gat_stats *stats,
-               std::chrono::steady_clock::time_point t0) {
+int run_clique(gat_executor *e, const DevGraphView &view, const std::vector<int64_t> &lo_host,
+               int k, int64_t ub, int64_t ue, cudaStream_t strm, bool balg, uint64_t *count,
+               gat_stats *stats, std::chrono::steady_clock::time_point t0) {
+    // roots whose units meet [ub, ue): from the one holding unit ub to the
+    // last one starting before ue
+    const int64_t vb = std::upper_bound(lo_host.begin(), lo_host.end(), ub) - lo_host.begin() - 1;
+    const int64_t ve = std::lower_bound(lo_host.begin(), lo_host.end(), ue) - lo_host.begin();
     int wocc = 0, cocc = 0;
     clique_blocks_per_sm(k, balg, &wocc, &cocc);
     if (wocc <= 0 || cocc <= 0) return fail(GAT_ERR_CUDA, "clique kernels do not fit on the device");
@@ -929,8 +933,10 @@ int run_clique(gat_executor *e, const DevGraphView &view, int k, int64_t vb, int
     CliqueLaunch L;
     L.g = view;
     L.k = k;
-    L.v_begin = vb;
-    L.v_end = ve;
+    L.v_begin = std::max<int64_t>(vb, 0);
+    L.v_end = std::min<int64_t>(ve, view.V);
+    L.u_begin = ub;
+    L.u_end = ue;
     L.warp_grid = warp_grid;
     L.cta_grid = cta_grid;
     L.ctr = e->ctr;
@@ -955,23 +961,17 @@ int run_clique(gat_executor *e, const DevGraphView &view, int k, int64_t vb, int
     st.kernel_ms = ms;
     st.raw_sum = raw;
     st.divisor = 1;
-    st.tasks = (uint64_t)(ve - vb);
+    st.tasks = (uint64_t)(ue - ub);
     st.balg_bytes = e->host_ctr->bytes;
     st.grid = cta_grid;
-    st.block = 256;
+    st.block = kCliqueCtaThreads;
     st.tile = 32;
-    st.launches = ve > vb ? 2 : 0;
+    st.launches = ue > ub ? 2 : 0;
     st.scratch_bytes = (int64_t)need;
     st.total_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (stats) *stats = st;
     return GAT_OK;
-}
-
-// First vertex v whose units start at or after unit u, units numbered by
-// the prefix sums `units` (V + 1 entries).
-int64_t first_root_at(const std::vector<int64_t> &units, int64_t u) {
-    return std::lower_bound(units.begin(), units.end() - 1, u) - units.begin();
 }
 
 int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *stream,
@@ -1048,18 +1048,11 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
     if (plan.special == GAT_SPECIAL_CLIQUE && s->mode == GAT_MODE_EXACT &&
         e->cfg.special_kernels == 1 && view.lo_off != nullptr &&
         view.max_lower <= kCliqueMaxLower) {
-        // Largest-vertex range of this call: whole graph, a root range, or
-        // the roots whose level-1 units (lower neighbours) start in the
-        // shard's unit range.
-        int64_t vb = 0, ve = view.V;
-        if (root_begin >= 0) {
-            vb = root_begin;
-            ve = root_end;
-        } else if (num_shards > 0) {
-            vb = first_root_at(dc->lo_host, shape.task_begin);
-            ve = shard + 1 == num_shards ? view.V : first_root_at(dc->lo_host, shape.task_end);
-        }
-        return run_clique(e, view, plan.n, vb, ve, strm, balg, count, stats, t0);
+        // The level-1 units of this call (whole graph, root range or shard),
+        // exactly as the plan path numbers them.
+        const int64_t ub = ranged ? shape.task_begin : 0;
+        const int64_t ue = ranged ? shape.task_end : view.lo_total;
+        return run_clique(e, view, dc->lo_host, plan.n, ub, ue, strm, balg, count, stats, t0);
     }
     if (plan.special == GAT_SPECIAL_C4 && s->mode == GAT_MODE_EXACT &&
         e->cfg.special_kernels == 1) {

@@ -55,7 +55,7 @@ constexpr int kMaxWords = kMaxD / 32;
 constexpr int kWarpD = 64;              // roots up to this go to the warp kernel
 constexpr int kWarpPitch = 3;           // row pitch of the warp kernel's matrix
 constexpr int kWarpThreads = 256;
-constexpr int kCtaThreads = 256;
+constexpr int kCtaThreads = kCliqueCtaThreads;
 constexpr int kCtaWarps = kCtaThreads / 32;
 constexpr int kRowSmemWords = 22 * 1024;  // 88 KB of matrix rows in shared memory
 constexpr int kQueue = 64;
@@ -131,7 +131,8 @@ struct CliqueArgs {
     const int32_t *hub_slot;  // null: no bitmaps
     const uint32_t *bitmaps;
     int64_t bitmap_words;
-    int64_t v_begin, v_end;
+    int64_t v_begin, v_end;   // roots holding the units [u_begin, u_end)
+    int64_t u_begin, u_end;   // level-1 units (v0, L[i]) numbered by lo_off
     DevCounters *ctr;
     CliqueAux *aux;
     uint32_t *rows;       // CTA kernel: per-CTA matrix for roots too large for
@@ -140,6 +141,15 @@ struct CliqueArgs {
 
 __device__ __forceinline__ int32_t lower_degree(const CliqueArgs &a, int64_t v) {
     return (int32_t)(a.lo_off[v + 1] - a.lo_off[v]);
+}
+
+// Rows [*r0, *r1) of root v0 (d rows) are units of this launch: unit
+// lo_off[v0] + i is (v0, L[i]), and its cliques are row i's.
+__device__ __forceinline__ void unit_rows(const CliqueArgs &a, int64_t v0, int d, int *r0,
+                                          int *r1) {
+    const int64_t lb = a.lo_off[v0];
+    *r0 = (int)max((int64_t)0, a.u_begin - lb);
+    *r1 = (int)min((int64_t)d, a.u_end - lb);
 }
 
 // Words [0, words_below(i)) of R_i = { j < i : L[j] in N(L[i]) }.  One warp.
@@ -382,18 +392,22 @@ __global__ void __launch_bounds__(kWarpThreads) clique_warp_kernel(const CliqueA
             mine &= mine - 1;
             const int64_t v0 = base + r;
             const int d = __shfl_sync(kFull, dl, r);
+            int r0, r1;
+            unit_rows(a, v0, d, &r0, &r1);
+            r0 = max(r0, K - 2);  // row i needs K-2 members below it
+            if (r0 >= r1) continue;
             const int pitch = row_pitch(d);
             const int32_t *src = a.adj + a.off[v0];
-            for (int t = lane; t < d; t += 32) S.L[t] = __ldg(src + t);
-            if (STATS && lane == 0) bytes += 4ull * (unsigned)d;
+            for (int t = lane; t < r1; t += 32) S.L[t] = __ldg(src + t);
+            if (STATS && lane == 0) bytes += 4ull * (unsigned)r1;
             __syncwarp();
-            for (int i = 1; i < d; i++) build_row<STATS>(a, S.L, i, S.R + i * pitch, lane, bytes);
+            for (int i = 1; i < r1; i++) build_row<STATS>(a, S.L, i, S.R + i * pitch, lane, bytes);
             __syncwarp();
             if constexpr (K == 4) {
-                for (int i = 2; i < d; i++) pairs_push_row(pq, S.R, pitch, i, lane, c, words);
+                for (int i = r0; i < r1; i++) pairs_push_row(pq, S.R, pitch, i, lane, c, words);
                 pairs_flush(pq, S.R, pitch, lane, c, words);
             } else {
-                for (int i = K - 2; i < d; i++)
+                for (int i = r0; i < r1; i++)
                     c += count_row<K>(S.R, pitch, i, S.stack, S.Q, lane, words);
             }
         }
@@ -530,24 +544,28 @@ __global__ void __launch_bounds__(kCtaThreads) clique_cta_kernel(const CliqueArg
                 S.next_build = kCtaWarps;
                 S.next_count = kCtaWarps;
             }
+            // rows below r1 are built; rows [r0, r1) are counted
+            int r0, r1;
+            unit_rows(a, v0, d, &r0, &r1);
+            r0 = max(r0, K - 2);
             __syncthreads();
             for (int i = wid;;) {
-                if (i >= d) break;
+                if (i >= r1) break;
                 build_row<STATS>(a, L, i, R + (int64_t)i * pitch, lane, bytes);
                 int nx = 0;
                 if (lane == 0) nx = atomicAdd(&S.next_build, 1);
                 i = __shfl_sync(kFull, nx, 0);
             }
             __syncthreads();
-            for (int i = wid;;) {
-                if (i >= d) break;
+            for (int i = r0 + wid;;) {
+                if (i >= r1) break;
                 if constexpr (K == 4)
                     pairs_push_row(pq, R, pitch, i, lane, c, words);
-                else if (i >= K - 2)
+                else
                     c += count_row<K>(R, pitch, i, S.stack[wid], S.Q[wid], lane, words);
                 int nx = 0;
                 if (lane == 0) nx = atomicAdd(&S.next_count, 1);
-                i = __shfl_sync(kFull, nx, 0);
+                i = r0 + __shfl_sync(kFull, nx, 0);
             }
             if constexpr (K == 4) pairs_flush(pq, R, pitch, lane, c, words);
             __syncthreads();
@@ -626,7 +644,7 @@ cudaError_t launch_clique(const CliqueLaunch &L, cudaStream_t st) {
         (e = cudaMemsetAsync(L.aux, 0, sizeof(CliqueAux), st)) != cudaSuccess)
         return e;
     CliqueArgs a{g.off, g.adj, g.lo_off, g.hub_slot, g.bitmaps, g.bitmap_words,
-                 L.v_begin, L.v_end, L.ctr, L.aux, L.rows, L.rows_stride};
+                 L.v_begin, L.v_end, L.u_begin, L.u_end, L.ctr, L.aux, L.rows, L.rows_stride};
     if (L.v_end <= L.v_begin) return cudaSuccess;
     switch (L.k * 2 + (L.stats ? 1 : 0)) {
         case 8: return launch_k<4, false>(a, L.warp_grid, L.cta_grid, st);

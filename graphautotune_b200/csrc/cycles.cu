@@ -246,13 +246,26 @@ __device__ __forceinline__ int32_t expand_group(RootSmem<BLOCK> &S, const int32_
     S.seg_base[threadIdx.x] = base;
     if (threadIdx.x == 0) S.pref[BLOCK] = total;
     __syncthreads();
+    // The segment holding flattened entry j is the last s with pref[s] <= j.
+    // A thread's entries grow by BLOCK per step, so its segment only moves
+    // forward: gallop from the previous one (one comparison while the
+    // segment lasts) and narrow the last step by bisection.
+    int32_t lo = 0;
     for (int32_t j = threadIdx.x; j < total; j += BLOCK) {
-        // the segment holding flattened entry j: last s with pref[s] <= j
-        int32_t lo = 0, n = BLOCK;
+        int32_t step = 1;
+        while (lo + step < BLOCK && S.pref[lo + step] <= j) {
+            lo += step;
+            step <<= 1;
+        }
+        int32_t n = min(lo + step, BLOCK) - lo;
         while (n > 1) {
             const int32_t h = n >> 1;
-            lo = (S.pref[lo + h] <= j) ? lo + h : lo;
-            n -= h;
+            if (S.pref[lo + h] <= j) {
+                lo += h;
+                n -= h;
+            } else {
+                n = h;
+            }
         }
         f(__ldg(adj + S.seg_base[lo] + (j - S.pref[lo])));
     }

@@ -91,13 +91,16 @@ int c4_light_blocks_per_sm(bool stats);
 int c4_root_blocks_per_sm(bool wide, bool stats);
 cudaError_t launch_c4(const C4Launch &launch, cudaStream_t st);
 
-// Exact k-clique count (4 <= k <= 7) over largest-id vertices [v_begin, v_end)
-// (plans with special == GAT_SPECIAL_CLIQUE) by bit-matrix induced subgraphs
+// Exact k-clique count (4 <= k <= 7) over the level-1 units [u_begin, u_end)
+// of the K_k exact plan: unit lo_off[v0] + i is (v0, i-th lower neighbour),
+// whose cliques have v0 as largest and that neighbour as second largest
+// vertex (plans with special == GAT_SPECIAL_CLIQUE), by bit-matrix induced subgraphs
 // of each root's lower list (cliques.cu).  Needs lo_off, every lower list of
 // at most kCliqueMaxLower entries, and adj readable 4 ints past its end.
 // `rows` holds cta_grid slices of rows_stride words when
 // clique_rows_words(max lower degree) > 0, else it may be null.
 constexpr int kCliqueMaxLower = 2048;
+constexpr int kCliqueCtaThreads = 512;  // threads of the CTA-per-root kernel
 struct CliqueAux {
     unsigned long long warp_cursor;
     unsigned long long cta_cursor;
@@ -106,7 +109,8 @@ struct CliqueAux {
 struct CliqueLaunch {
     DevGraphView g;
     int k = 4;
-    int64_t v_begin = 0, v_end = 0;
+    int64_t v_begin = 0, v_end = 0;  // roots holding the units [u_begin, u_end)
+    int64_t u_begin = 0, u_end = 0;  // level-1 units (v0, v1 < v0) numbered by lo_off
     int warp_grid = 0, cta_grid = 0;
     DevCounters *ctr = nullptr;
     CliqueAux *aux = nullptr;

@@ -327,7 +327,7 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64):
         if t_default > 20000:
             emit(config="c5", pattern=name, skipped="slice too slow")
             continue
-        picked = costmodel.pick(model, gf, pf, cands)
+        picked, kept_default = costmodel.choose(model, gf, pf, cands, default)
         raw_p, t_pick = measure(picked)
         times = []
         for d in cands:
@@ -345,6 +345,7 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64):
              model_pick_ms=t_pick, best_measured_ms=times[best],
              median_candidate_ms=float(np.median(times)),
              pick_vs_default=t_default / t_pick, pick_vs_best=times[best] / t_pick,
+             kept_default=kept_default,
              spearman_pred_vs_measured=rank_corr, candidates=len(cands_m),
              picked={k.split(".")[-1]: v for k, v in picked.items()},
              best={k.split(".")[-1]: v for k, v in cands[best].items()})

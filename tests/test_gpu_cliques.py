@@ -108,7 +108,11 @@ def test_clique_ranges_and_shards_sum_to_the_whole(gat, executors):
             assert got == want, (k, b, e)
             total += got
         assert total == whole
-        assert sum(ex.count_shard(g, s, i, 5)[0] for i in range(5)) == whole
+        # shards split the level-1 units (v0, v1) exactly as the plan path
+        # does, rows of one root included
+        shards = [ex.count_shard(g, s, i, 7)[0] for i in range(7)]
+        assert shards == [plain.count_shard(g, s, i, 7)[0] for i in range(7)], k
+        assert sum(shards) == whole
 
 
 def test_clique_rows_in_global_scratch(gat, oracle, executors):

@@ -3,10 +3,11 @@
   * gradients of gat_mlp_gradient equal the float64 numpy restatement
     (oracle/mlp_ref.py) for random parameters and data
   * Adam training on the GPU fits a known smooth function
-  * trained on engine timings from some graphs, the network's pick of a launch
-    configuration on held-out graphs runs faster than a configuration chosen
-    without it (the mean over the candidate set, i.e. a random pick), and its
-    predicted order correlates with the measured one
+  * trained on engine timings from some graphs, the network's choice of a
+    launch configuration on held-out graphs (with the default configuration
+    as its fallback) is judged against the default configuration and against
+    the best measured candidate; its predicted order correlates with the
+    measured one
 """
 import math
 import random
@@ -59,8 +60,10 @@ def test_trained_model_beats_choosing_without_it(gat):
         gr = make_graph(sp)
         gr.upload(degree_order=True)
         graphs.append((gr, costmodel.graph_features(gr)))
-    pats = ["0111101111011110", "0101101001011010", "0100110110010110110010100",
-            "0111110111110111110111110"]
+    # patterns counted by the schedule-plan interpreter, whose launch shape
+    # matters (the 4-cycle and cliques have dedicated kernels): the house,
+    # the diamond and the tailed triangle
+    pats = ["0100110110010110110010100", "0111101111001100", "0111101011001000"]
     scheds = [gat.Schedule(p, "exact") for p in pats]
     pfs = [costmodel.plan_features(s) for s in scheds]
     rng = random.Random(0)
@@ -73,7 +76,7 @@ def test_trained_model_beats_choosing_without_it(gat):
     for c in cfgs:
         c.memory_budget = costmodel.EXEC_BUDGET
     execs = [gat.Executor(c) for c in cfgs]
-    groups = []  # (graph index, X rows, measured ms)
+    groups = []  # (graph index, pattern index, X rows, measured ms)
     for gi, (gr, gf) in enumerate(graphs):
         for si, s in enumerate(scheds):
             times = []
@@ -81,20 +84,34 @@ def test_trained_model_beats_choosing_without_it(gat):
                 ex.count(gr, s)
                 times.append(min(ex.count(gr, s).kernel_ms for _ in range(2)))
             X = np.stack([costmodel.features(gf, pfs[si], d) for d in cands])
-            groups.append((gi, X, np.array(times)))
+            groups.append((gi, si, X, np.array(times)))
     train = [x for x in groups if x[0] < 7]
     test = [x for x in groups if x[0] >= 7]
-    Xtr = np.concatenate([x[1] for x in train])
-    Ttr = np.log(np.concatenate([x[2] for x in train])).astype(np.float32)
+    Xtr = np.concatenate([x[2] for x in train])
+    Ttr = np.log(np.concatenate([x[3] for x in train])).astype(np.float32)
     model, _ = costmodel.CostModel.fit(Xtr, Ttr, epochs=300, seed=0, lr=2e-3)
-    gains, corrs = [], []
-    for _, X, times in test:
+    vs_default, vs_best, corrs, kept = [], [], [], 0
+    fps = [tuner.fingerprint(d) for d in cands]
+    for gi, si, X, times in test:
+        choice, k = costmodel.choose(model, graphs[gi][1], pfs[si], cands, cands[0])
+        kept += k
+        t = times[fps.index(tuner.fingerprint(choice))]
+        vs_default.append(times[0] / t)
+        vs_best.append(float(times.min()) / t)
         pred = model.predict(X)
-        pick = int(np.argmin(pred))
-        gains.append(float(np.mean(times)) / times[pick])
         corrs.append(float(np.corrcoef(np.argsort(np.argsort(pred)),
                                        np.argsort(np.argsort(times)))[0, 1]))
-    # geometric-mean gain of the model's pick over a pick made without it
-    gm = math.exp(sum(math.log(x) for x in gains) / len(gains))
-    assert gm > 1.1, (gains, corrs)
-    assert float(np.mean(corrs)) > 0.3, corrs
+
+    def gm(xs):
+        return math.exp(sum(math.log(x) for x in xs) / len(xs))
+
+    info = dict(vs_default=gm(vs_default), vs_best=gm(vs_best), kept_default=kept,
+                groups=len(test), corr=float(np.mean(corrs)))
+    print(info)
+    # the choice is not slower than the default (geometric mean over the
+    # held-out graph x pattern groups; measured 2.25x faster), it keeps at
+    # least half the best measured candidate's speed (measured 0.66), and the
+    # predicted order follows the measured one (measured 0.93)
+    assert info["vs_default"] >= 1.0, info
+    assert info["vs_best"] >= 0.5, info
+    assert info["corr"] > 0.5, info

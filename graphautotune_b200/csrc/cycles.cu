@@ -28,7 +28,10 @@
 //    flattened with a block scan so that consecutive threads read
 //    consecutive list entries, the counters are incremented with shared
 //    atomics, and the window's counters are read, summed as C(c, 2) and
-//    cleared before the next window.
+//    cleared before the next window.  Once the wedges left fit the CTA
+//    table, the lists' remainders go through the table in one pass (the
+//    endpoints crowd the low, high-degree ids: on R-MAT most heavy roots
+//    need one window and the table).
 //
 // Neither kernel waits on another CTA; the deferred list is written by the
 // first launch and read by the second, ordered on the stream.
@@ -375,6 +378,44 @@ __global__ void __launch_bounds__(BLOCK, 1) c4_root_kernel(const RootArgs a) {
         for (int i = threadIdx.x; i < kRegionWords; i += BLOCK) region[i] = 0u;
         long long left = Wall;
         for (int64_t xlo = v0 + 1; xlo < a.V && left > 0; xlo += kWindow) {
+            if (left <= kCtaWedges) {
+                // The rest fits the CTA table (wedge endpoints crowd the low,
+                // high-degree ids, so this is usually after the first
+                // window): one pass over every list's remainder.
+                __syncthreads();
+                for (int i = threadIdx.x; i < kCtaSlots; i += BLOCK) {
+                    tkey[i] = kEmpty;
+                    tcnt[i] = 0;
+                }
+                for (int g = 0; g < ngroups; g++) {
+                    const int i = g * BLOCK + threadIdx.x;
+                    int64_t base = 0;
+                    int32_t len = 0;
+                    if (i < dp) {
+                        if (ngroups == 1) {
+                            base = my_o1 + my_pos;
+                            len = my_end - my_pos;
+                        } else {
+                            const int32_t v1 = U[i];
+                            const int64_t o1 = a.off[v1];
+                            base = o1 + cur[i];
+                            len = (int32_t)(a.off[v1 + 1] - o1) - cur[i];
+                        }
+                    }
+                    expand_group<BLOCK>(S, a.adj, base, len, [&](int32_t x) {
+                        table_add(tkey, tcnt, 14, x, &a.ctr->error);
+                    });
+                }
+                __syncthreads();
+                for (int s = threadIdx.x; s < kCtaSlots; s += BLOCK) {
+                    if (tkey[s] != kEmpty) {
+                        part += pairs_of(tcnt[s]);
+                        tkey[s] = kEmpty;
+                        tcnt[s] = 0;
+                    }
+                }
+                break;
+            }
             const int32_t xhi = (int32_t)(xlo + kWindow < (int64_t)a.V ? xlo + kWindow : (int64_t)a.V);
             int32_t in_window = 0;
             for (int g = 0; g < ngroups; g++) {

@@ -267,11 +267,12 @@ def _bipartite_with_ring(gat, n: int):
 def test_four_cycle_kernel_paths(gat, oracle):
     """The 4-cycle kernels' paths: warp tables for light roots, roots
     deferred to the CTA table, CTA windows over the ids (one window on a
-    dense graph, several when V exceeds a window), roots with more upper
-    neighbours than a CTA has threads, 32-bit window counters when a pair of
-    vertices shares 2^16 or more neighbours, odd V; repeated calls with one
-    executor across graphs, and shards.  Each count equals the host oracle's
-    count at each cycle's largest vertex and the schedule plan's."""
+    dense graph, several when V exceeds a window), the tail of a root's
+    wedges through the CTA table, roots with more upper neighbours than a
+    CTA has threads (up to 15,544 on the scale-17 R-MAT), 32-bit window
+    counters when a pair of vertices shares 2^16 or more neighbours, odd V;
+    repeated calls with one executor across graphs, and shards.  Each count equals the host oracle's count at each
+    cycle's largest vertex and the schedule plan's."""
     c4 = "0101101001011010"
     s = gat.Schedule(c4, "exact")
     plan = _executor(gat, special_kernels=0)
@@ -279,7 +280,8 @@ def test_four_cycle_kernel_paths(gat, oracle):
              gat.Graph.barabasi_albert(120000, 12, 12),
              gat.Graph.rmat(14, 1 << 17, 0.57, 0.19, 0.19, 13),
              gat.Graph.barabasi_albert(3001, 8, 21),
-             _bipartite_with_ring(gat, 70000)]
+             _bipartite_with_ring(gat, 70000),
+             gat.Graph.rmat(17, 1 << 21, 0.57, 0.19, 0.19, 17)]
     assert cases[1].info()[2] > 1024 and cases[4].info()[2] >= 1 << 16
     wants = []
     for g in cases:

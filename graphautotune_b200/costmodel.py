@@ -30,7 +30,7 @@ from graphautotune_b200 import tuner
 from graphautotune_b200._lib import check, lib
 
 HIST_BUCKETS = 15
-N_FEATURES = 7 + 10 + 5 + HIST_BUCKETS
+N_FEATURES = 7 + 11 + 5 + HIST_BUCKETS
 
 
 def _bind():
@@ -137,13 +137,14 @@ def graph_features(graph: "g.Graph") -> np.ndarray:
 def plan_features(sched: "g.Schedule") -> np.ndarray:
     raw = sched.plan_bytes()
     i32 = np.frombuffer(raw[:40], np.int32)
-    n, basic, num_prefix, mode, collide, l1b, num_store, iep_num, num_terms = i32[:9]
+    n, basic, num_prefix, mode, collide, l1b, num_store, iep_num, num_terms, special = i32[:10]
     divisor = np.frombuffer(raw[40:48], np.int64)[0]
     kinds = np.frombuffer(raw[48 + 64:48 + 96], np.int8)[:num_prefix]
     edges = sched.pattern.adjacency().count("1") // 2
     return np.array([n / 10, basic / 10, num_prefix / 16, num_store / 8, iep_num / 8,
                      num_terms / 16, math.log2(max(int(divisor), 1)) / 10, float(l1b),
-                     float((kinds == 2).sum()) / 8, edges / 45], np.float32)
+                     float((kinds == 2).sum()) / 8, edges / 45,
+                     float(special != 0)], np.float32)
 
 
 def config_features(d: dict) -> np.ndarray:
@@ -185,10 +186,14 @@ def training_graphs(count: int, seed0: int = 1000, max_log2: int = 16) -> list[d
 
 
 def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
-            log=None, max_seconds: float = 0.0, max_log2: int = 16
+            log=None, max_seconds: float = 0.0, max_log2: int = 16,
+            checkpoint: str | None = None, every: int = 500
             ) -> tuple[np.ndarray, np.ndarray]:
     """Times `runs` random (graph, pattern, configuration) counts (fewer if
-    `max_seconds` > 0 runs out first)."""
+    `max_seconds` > 0 runs out first).  With `checkpoint`, the rows gathered
+    so far are saved there every `every` runs, and a run that finds the file
+    keeps its rows and adds new ones (drawn from a stream seeded by the
+    seed and the number of rows already there)."""
     from graphautotune_b200.experiments import make_graph
 
     rng = random.Random(seed)
@@ -201,6 +206,15 @@ def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
     scheds = [g.Schedule(p, "exact") for p in pats]
     pfs = [plan_features(s) for s in scheds]
     X, T = [], []
+    if checkpoint:
+        import os
+
+        if os.path.exists(checkpoint):
+            z = np.load(checkpoint)
+            X, T = list(z["X"]), list(z["T"])
+            rng = random.Random(seed * 1000003 + len(X))
+            if log:
+                log(f"resumed {len(X)} runs from {checkpoint}")
     # a few executors at a time (each keeps its scratch), with a modest
     # memory budget: thousands of random configurations are visited
     from collections import OrderedDict
@@ -227,8 +241,12 @@ def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
             slow.add((gi, si))  # keep the data set cheap to gather
         X.append(features(gf, pfs[si], d))
         T.append(math.log(max(r.kernel_ms, 1e-3)))
+        if checkpoint and len(X) % every == 0:
+            np.savez(checkpoint, X=np.stack(X), T=np.array(T, np.float32))
         if log and len(X) % 1000 == 0:
             log(f"collected {len(X)} runs in {time.time() - t0:.1f}s")
+    if checkpoint and X:
+        np.savez(checkpoint, X=np.stack(X), T=np.array(T, np.float32))
     return np.stack(X), np.array(T, np.float32)
 
 
@@ -349,7 +367,8 @@ def main():
     torch.cuda.set_device(0)
     if a.cmd == "collect":
         X, T = collect(a.runs, a.seed, log=lambda s: print(s, file=sys.stderr, flush=True),
-                       max_seconds=a.max_seconds, max_log2=a.max_log2, max_ms=a.max_ms)
+                       max_seconds=a.max_seconds, max_log2=a.max_log2, max_ms=a.max_ms,
+                       checkpoint=a.out)
         np.savez(a.out, X=X, T=T)
         print(json.dumps({"runs": len(X), "features": X.shape[1], "out": a.out}))
     elif a.cmd == "train":

@@ -6,8 +6,13 @@
     python -m graphautotune_b200.experiments c4 [--tune N]
                                                      # 21 patterns x 64 graphs: plain
                                                      # launches vs one batched launch
+    python -m graphautotune_b200.experiments c5 [--model cm.npz]
+                                                     # R-MAT 2^24: 6-clique in full, the
+                                                     # other two patterns on slices with
+                                                     # cost-model picks
 
-Graphs are synthetic and seeded (splitmix64 streams in libgat).
+Graphs are synthetic and seeded (splitmix64 streams in libgat), built on the
+device.
 """
 from __future__ import annotations
 
@@ -52,10 +57,11 @@ def c4_graph_spec(seed: int) -> dict:
     return {"seed": seed, "kind": "ba", "n": n, "m": int(m)}
 
 
-def make_graph(spec: dict) -> "g.Graph":
+def make_graph(spec: dict, device: bool = True) -> "g.Graph":
     if spec["kind"] == "rmat":
-        return g.Graph.rmat(spec["scale"], spec["samples"], 0.57, 0.19, 0.19, spec["seed"])
-    return g.Graph.barabasi_albert(spec["n"], spec["m"], spec["seed"])
+        return g.Graph.rmat(spec["scale"], spec["samples"], 0.57, 0.19, 0.19, spec["seed"],
+                            device=device)
+    return g.Graph.barabasi_albert(spec["n"], spec["m"], spec["seed"], device=device)
 
 
 def plain_config() -> "g.Config":
@@ -84,7 +90,7 @@ def run_c3(args):
     the full count's time; the full count runs when the estimate is below
     `--max-seconds`."""
     t0 = time.time()
-    gr = g.Graph.rmat(22, 1 << 26, 0.57, 0.19, 0.19, 3)
+    gr = g.Graph.rmat(22, 1 << 26, 0.57, 0.19, 0.19, 3, device=True)
     V, E, md = gr.info()
     gr.upload(degree_order=True)
     emit(config="c3", graph="R-MAT scale 22, 2^26 samples, seed 3", V=V, E=E, max_degree=md,
@@ -277,7 +283,7 @@ def c5_candidates() -> list[dict]:
     return out
 
 
-def eval_c5(model, parts: int = 256, n_candidates: int = 64):
+def eval_c5(model, parts: int = 256, n_candidates: int = 64, graph=None, names=None):
     """Configuration 5: the cost model picks a launch configuration for 6- and
     7-vertex patterns on R-MAT 2^24 (average degree 24, seed 4); compared with
     the default configuration and the best of the exhaustively measured
@@ -287,9 +293,11 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64):
     from graphautotune_b200 import costmodel, tuner
 
     t0 = time.time()
-    gr = g.Graph.rmat(24, 12 << 24, 0.57, 0.19, 0.19, 4)
+    gr = graph
+    if gr is None:
+        gr = g.Graph.rmat(24, 12 << 24, 0.57, 0.19, 0.19, 4, device=True)
+        gr.upload(degree_order=True)
     V, E, md = gr.info()
-    gr.upload(degree_order=True)
     gf = costmodel.graph_features(gr)
     emit(config="c5", graph="R-MAT scale 24, 12*2^24 samples (avg degree 24), seed 4", V=V,
          E=E, max_degree=md, setup_s=time.time() - t0)
@@ -301,6 +309,8 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64):
     if all(tuner.fingerprint(c) != tuner.fingerprint(default) for c in cands):
         cands = [default] + cands[:-1]
     for name, pat in C5_PATTERNS.items():
+        if names is not None and name not in names:
+            continue
         s = g.Schedule(pat, "exact", stats_graph=gr)
         pf = costmodel.plan_features(s)
         # The slice: the middle shard of P, P grown from `parts` until the
@@ -351,9 +361,38 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64):
              best={k.split(".")[-1]: v for k, v in cands[best].items()})
 
 
+def run_c5(args):
+    """R-MAT 2^24 (12 * 2^24 samples, average degree 24, seed 4): the
+    6-clique counted over the whole graph by the clique kernels (the launch
+    configuration does not enter them), then, with --model, the 6-cycle with
+    chord and the 7-vertex triangle + path on work-queue slices, where the
+    cost model picks the launch configuration and is compared with the
+    default and the best measured candidate (eval_c5)."""
+    t0 = time.time()
+    gr = g.Graph.rmat(24, 12 << 24, 0.57, 0.19, 0.19, 4, device=True)
+    t_gen = time.time() - t0
+    t0 = time.time()
+    gr.upload(degree_order=True)
+    V, E, md = gr.info()
+    emit(config="c5", graph="R-MAT scale 24, 12*2^24 samples (avg degree 24), seed 4", V=V,
+         E=E, max_degree=md, generate_on_device_s=t_gen, upload_s=time.time() - t0)
+    ex = g.Executor()
+    s = g.Schedule(C5_PATTERNS["k6"], "exact", stats_graph=gr)
+    r = ex.count(gr, s)
+    times = [ex.count(gr, s).kernel_ms for _ in range(2)]
+    emit(config="c5", pattern="k6", count=r.count, kernel_ms=min(times),
+         matches_per_s=r.count / (min(times) / 1e3), launches=r.launches,
+         kernel="clique kernels" if r.launches == 2 else "schedule plan")
+    if args.model:
+        from graphautotune_b200.costmodel import CostModel
+
+        eval_c5(CostModel.load(args.model), parts=args.parts, graph=gr,
+                names=["c6_chord", "tri_path_7v"])
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["c1", "c3", "c4"])
+    ap.add_argument("config", choices=["c1", "c3", "c4", "c5"])
     ap.add_argument("--graphs", type=int, default=64)
     ap.add_argument("--tune", type=int, default=0)
     ap.add_argument("--max-seconds", type=float, default=120.0)
@@ -369,7 +408,7 @@ def main():
     import torch
 
     torch.cuda.set_device(0)
-    {"c1": run_c1, "c3": run_c3, "c4": run_c4}[args.config](args)
+    {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args)
 
 
 if __name__ == "__main__":

@@ -108,7 +108,10 @@ def random_walk(d: dict, rng: random.Random) -> dict:
 
 
 class History:
-    """Measured (config, seconds) pairs, persisted as record.json."""
+    """Measured (config, seconds) pairs, persisted as record.json; the best
+    pair so far goes to best_config.json beside it (the file the reference's
+    tuner names as CONF_PATH, tuning/tuning/common/const.py:27-30), as
+    [value dict, seconds] like one record entry."""
 
     def __init__(self, path: str | None = None):
         self.path = Path(path) if path else None
@@ -125,6 +128,8 @@ class History:
         if self.path:
             self.path.parent.mkdir(parents=True, exist_ok=True)
             self.path.write_text(json.dumps([[a, b] for a, b in zip(self.xs, self.ys)]))
+            bx, by = self.best()
+            (self.path.parent / "best_config.json").write_text(json.dumps([bx, by]))
 
     def seen(self, x: dict) -> bool:
         f = fingerprint(x)

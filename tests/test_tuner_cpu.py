@@ -52,6 +52,10 @@ def test_history_persists_as_record_json(tuner, tmp_path):
     h2 = tuner.History(str(path))
     assert h2.best() == (pts[0], 1.0)
     assert all(h2.seen(p) for p in pts)
+    # best_config.json (the reference tuner's CONF_PATH) holds the best pair
+    assert json.loads((path.parent / "best_config.json").read_text()) == [pts[0], 1.0]
+    h2.add(pts[1], 0.5)
+    assert json.loads((path.parent / "best_config.json").read_text()) == [pts[1], 0.5]
 
 
 def _bowl(tuner):
@@ -109,7 +113,9 @@ def test_feature_vectors(gat):
     assert gf.shape == (20,) and np.all(np.isfinite(gf))
     for p in ("0111101111011110", "0100110110010110110010100"):
         pf = costmodel.plan_features(gat.Schedule(p, "exact"))
-        assert pf.shape == (10,) and np.all(np.isfinite(pf))
+        assert pf.shape == (11,) and np.all(np.isfinite(pf))
+        # the last plan feature flags a dedicated kernel (the 4-clique's)
+        assert pf[-1] == (1.0 if p == "0111101111011110" else 0.0)
         x = costmodel.features(gf, pf, tuner.default_point())
         assert x.shape == (costmodel.N_FEATURES,) and np.all(np.isfinite(x))
     pts = costmodel.all_points()

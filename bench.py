@@ -553,17 +553,22 @@ def run_ours(args):
         off, adj = gr.csr()
         off_p = torch.from_numpy(off).pin_memory()
         adj_p = torch.from_numpy(adj).pin_memory()
-        e2e_ms = []
+        e2e_ms, parts_ms = [], []
         for i in range(max(1, min(3, args.steps))):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             g2 = g.Graph.from_csr(off_p.numpy(), adj_p.numpy(), check_symmetry=False)
+            t1 = time.perf_counter()
             g2.upload(degree_order=True)
+            t2 = time.perf_counter()
             tot = 0
             for k, s in scheds.items():
                 tot += ex.count(g2, s).count
             torch.cuda.synchronize()
-            e2e_ms.append((time.perf_counter() - t0) * 1000)
+            t3 = time.perf_counter()
+            e2e_ms.append((t3 - t0) * 1000)
+            parts_ms.append({"graph_from_host_arrays": (t1 - t0) * 1000,
+                             "upload": (t2 - t1) * 1000, "counts": (t3 - t2) * 1000})
             assert tot == matches, (tot, matches)
             del g2
         e2e_value = matches / (statistics.median(e2e_ms) / 1000.0)
@@ -590,7 +595,8 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "matches/s",
                     "h2d_bytes_per_step": int(off.nbytes + adj.nbytes),
                     "d2h_bytes_per_step": 32 * len(PATTERNS), "ms_per_step":
-                    statistics.median(e2e_ms)},
+                    statistics.median(e2e_ms),
+                    "breakdown_ms": parts_ms},
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,

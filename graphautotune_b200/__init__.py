@@ -127,6 +127,17 @@ class Schedule(_Handle):
         check(lib().gat_schedule_plan(self._h, buf, need.value, C.byref(need)))
         return buf.raw
 
+    @property
+    def dedicated_kernel(self) -> int:
+        """The device plan's `special` field: 0 when the plan interpreter
+        counts it, 1 for the 4-cycle's wedge kernels, 2 for the clique
+        kernels (exact mode; Executor counts use them unless
+        Config.special_kernels says otherwise; batched launches interpret
+        the plan)."""
+        import struct
+
+        return struct.unpack_from("<i", self.plan_bytes(), 36)[0]
+
 
 @dataclass
 class Config:

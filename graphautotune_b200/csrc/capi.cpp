@@ -96,6 +96,12 @@ struct gat_graph {
     DevCopy dev;          // ids as given
     DevCopy dev_ordered;  // relabelled by decreasing degree
     int device = -1;
+    // Hub bitmap parameters of the last upload.  With the degree-ordered
+    // copy present, the given-id copy's bitmaps (used only by
+    // reference-compatible counts) are built on first use.
+    int64_t hub_min_degree = GAT_HUB_MIN_DEGREE_DEFAULT;
+    int64_t hub_max_bytes = GAT_HUB_MAX_BYTES_DEFAULT;
+    bool dev_hubs_pending = false;
     ~gat_graph() {
         dev.release();
         dev_ordered.release();
@@ -644,6 +650,13 @@ int upload_hubs(DevCopy &d, int32_t V, int64_t min_degree, int64_t max_bytes,
     d.bitmap_words = words;
     return GAT_OK;
 }
+
+// Builds the given-id copy's hub bitmaps if the last upload deferred them.
+int ensure_dev_hubs(gat_graph *g, cudaStream_t st) {
+    if (!g->dev_hubs_pending || !g->dev.ready) return GAT_OK;
+    g->dev_hubs_pending = false;
+    return upload_hubs(g->dev, g->host.V, g->hub_min_degree, g->hub_max_bytes, st);
+}
 }  // namespace
 
 int gat_graph_generate_device(int kind, double p0, double p1, double p2, double p3, double p4,
@@ -734,7 +747,11 @@ int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
         release_hubs(g->dev);
     else
         rc = upload_copy(g->host, g->dev, st);
-    if (rc == GAT_OK) rc = upload_hubs(g->dev, V, hub_min_degree, hub_max_bytes, st);
+    g->hub_min_degree = hub_min_degree;
+    g->hub_max_bytes = hub_max_bytes;
+    g->dev_hubs_pending = (flags & GAT_UPLOAD_DEGREE_ORDER) != 0;
+    if (rc == GAT_OK && !g->dev_hubs_pending)
+        rc = upload_hubs(g->dev, V, hub_min_degree, hub_max_bytes, st);
     if (rc != GAT_OK) return rc;
     if (flags & GAT_UPLOAD_DEGREE_ORDER) {
         if (g->dev_ordered.ready && g->device == dev) {
@@ -760,6 +777,11 @@ int gat_graph_upload(gat_graph *g, int flags, void *stream) {
 
 int gat_graph_hubs(const gat_graph *g, int ordered_copy, int32_t *nhubs) {
     if (!g || !nhubs) return fail(GAT_ERR_ARGUMENT, "null argument");
+    if (!ordered_copy) {
+        // the given-id copy's bitmaps may still be pending: build them now
+        int rc = ensure_dev_hubs(const_cast<gat_graph *>(g), nullptr);
+        if (rc != GAT_OK) return rc;
+    }
     *nhubs = ordered_copy ? g->dev_ordered.nhubs : g->dev.nhubs;
     return GAT_OK;
 }
@@ -1005,6 +1027,8 @@ int count_impl(gat_executor *e, gat_graph *g, const gat_schedule *s, void *strea
             int rc = gat_graph_upload(g, 0, stream);
             if (rc != GAT_OK) return rc;
         }
+        int rc = ensure_dev_hubs(g, strm);
+        if (rc != GAT_OK) return rc;
         dc = &g->dev;
     }
     DevGraphView view;
@@ -1320,6 +1344,10 @@ int gat_batch_prepare(gat_batch *b, const gat_config *c, int use_cuda_graph) {
         const bool exact = s->mode == GAT_MODE_EXACT;
         if (!g->dev.ready || (exact && !g->dev_ordered.ready)) {
             int rc = gat_graph_upload(g, exact ? GAT_UPLOAD_DEGREE_ORDER : 0, b->stream);
+            if (rc != GAT_OK) return rc;
+        }
+        if (!(exact && g->dev_ordered.ready)) {
+            int rc = ensure_dev_hubs(g, b->stream);
             if (rc != GAT_OK) return rc;
         }
         const DevCopy &dc = (exact && g->dev_ordered.ready) ? g->dev_ordered : g->dev;

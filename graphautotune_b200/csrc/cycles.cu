@@ -249,12 +249,18 @@ __device__ __forceinline__ int32_t expand_group(RootSmem<BLOCK> &S, const int32_
     S.seg_base[threadIdx.x] = base;
     if (threadIdx.x == 0) S.pref[BLOCK] = total;
     __syncthreads();
-    // The segment holding flattened entry j is the last s with pref[s] <= j.
-    // A thread's entries grow by BLOCK per step, so its segment only moves
-    // forward: gallop from the previous one (one comparison while the
-    // segment lasts) and narrow the last step by bisection.
+    // Each warp takes one contiguous block of the flattened entries, its
+    // lanes on consecutive entries (coalesced reads), so a lane's next entry
+    // is 32 further on.  The segment holding entry j is the last s with
+    // pref[s] <= j; it only moves forward, so the lane gallops from its
+    // previous segment (one comparison while the segment lasts) and narrows
+    // the last step by bisection.
+    constexpr int kWarps = BLOCK / 32;
+    const int32_t per = (total + kWarps - 1) / kWarps;
+    const int32_t jb = (int32_t)(threadIdx.x >> 5) * per;
+    const int32_t je = min(total, jb + per);
     int32_t lo = 0;
-    for (int32_t j = threadIdx.x; j < total; j += BLOCK) {
+    for (int32_t j = jb + (int32_t)(threadIdx.x & 31); j < je; j += 32) {
         int32_t step = 1;
         while (lo + step < BLOCK && S.pref[lo + step] <= j) {
             lo += step;

@@ -182,6 +182,86 @@ __device__ __forceinline__ bool contains(const int32_t *b, int nb, int32_t x,
     return b[lo] == x;
 }
 
+// Merge-based intersection for balanced pairs: binary search costs
+// |A| log |B| probes, a merge |A| + |B| steps.  Lane l of the tile owns the
+// block [l |A| / G, (l + 1) |A| / G) of the shorter list A, finds where the
+// block starts in B by one binary search and walks both lists from there, so
+// every common element is found once, by the lane owning it in A.
+__device__ __forceinline__ bool merge_pays(int shorter, int longer) {
+    int lg = 1;
+    while ((1 << lg) < longer + 1) lg++;
+    return (long long)shorter * lg > 2ll * (shorter + longer);
+}
+
+// First i in a[0, n) with a[i] >= x (one lane alone).
+__device__ __forceinline__ int lower_index(const int32_t *a, int n, int32_t x) {
+    int lo = 0;
+    while (n > 0) {
+        const int h = n >> 1;
+        const bool right = a[lo + h] < x;
+        lo = right ? lo + h + 1 : lo;
+        n = right ? n - h - 1 : h;
+    }
+    return lo;
+}
+
+// Common elements of a[i0, i1) and b[j, nb) (both sorted), in order: f(x)
+// for each.  One lane alone.
+template <class F>
+__device__ __forceinline__ void merge_walk(const int32_t *a, int i0, int i1, const int32_t *b,
+                                           int nb, F &&f) {
+    if (i0 >= i1) return;
+    int i = i0, j = lower_index(b, nb, a[i0]);
+    while (i < i1 && j < nb) {
+        const int32_t x = a[i], y = b[j];
+        if (x == y) f(x);
+        i += x <= y ? 1 : 0;
+        j += y <= x ? 1 : 0;
+    }
+}
+
+template <int G>
+__device__ __forceinline__ int merge_count(const Tile<G> &t, const int32_t *a, int na,
+                                           const int32_t *b, int nb, const TileSmem &S,
+                                           unsigned excl) {
+    const int i0 = (int)((long long)na * t.lane / G), i1 = (int)((long long)na * (t.lane + 1) / G);
+    int c = 0;
+    merge_walk(a, i0, i1, b, nb, [&](int32_t x) {
+        bool ok = true;
+        unsigned m = excl;
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            ok &= (S.v[j] != x);
+        }
+        c += ok ? 1 : 0;
+    });
+    return t.sum(c);
+}
+
+// Stored merge: a counting walk, an exclusive scan of the lanes' counts,
+// and a writing walk (outputs in order, at most `cap` kept).
+template <int G>
+__device__ __forceinline__ int merge_store(const Tile<G> &t, const int32_t *a, int na,
+                                           const int32_t *b, int nb, int32_t *out, int cap) {
+    const int i0 = (int)((long long)na * t.lane / G), i1 = (int)((long long)na * (t.lane + 1) / G);
+    int c = 0;
+    merge_walk(a, i0, i1, b, nb, [&](int32_t) { c++; });
+    int at = c;
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) {
+        const int y = __shfl_up_sync(t.mask, at, o, G);
+        if (t.lane >= o) at += y;
+    }
+    const int total = t.bcast(at, G - 1);
+    at -= c;
+    merge_walk(a, i0, i1, b, nb, [&](int32_t x) {
+        if (at < cap) out[at] = x;
+        at++;
+    });
+    return total;
+}
+
 template <int G>
 __device__ __forceinline__ int isect_count(const Tile<G> &t, const int32_t *a,
                                            int na, const int32_t *b, int nb,
@@ -195,6 +275,8 @@ __device__ __forceinline__ int isect_count(const Tile<G> &t, const int32_t *a,
         na = nb;
         nb = tn;
     }
+    if (G > 1 && nb >= linear_below && merge_pays(na, nb))
+        return merge_count(t, a, na, b, nb, S, excl);
     int c = 0;
     for (int i = t.lane; i < na; i += G) {
         const int32_t x = a[i];
@@ -225,6 +307,8 @@ __device__ __forceinline__ int isect_store(const Tile<G> &t, const int32_t *a,
         na = nb;
         nb = tn;
     }
+    if (G > 1 && nb >= linear_below && merge_pays(na, nb))
+        return merge_store(t, a, na, b, nb, out, cap);
     int n = 0;
     for (int base = 0; base < na; base += G) {
         const int i = base + t.lane;
@@ -593,12 +677,18 @@ __device__ unsigned long long lane_last_level(const Tile<G> &t, const TileSmem &
                 const int32_t *sa = nl <= fl ? nb : fp;
                 const int32_t *lb = nl <= fl ? fp : nb;
                 const int ns = min(nl, fl), nlong = max(nl, fl);
-                for (int e = 0; e < ns; e++) {
-                    const int32_t y = sa[e];
-                    c += (contains(lb, nlong, y, a.linear_below) &&
-                          !excluded(S, ex, k, cand, y))
-                             ? 1
-                             : 0;
+                if (nlong >= a.linear_below && merge_pays(ns, nlong)) {
+                    merge_walk(sa, 0, ns, lb, nlong, [&](int32_t y) {
+                        c += excluded(S, ex, k, cand, y) ? 0 : 1;
+                    });
+                } else {
+                    for (int e = 0; e < ns; e++) {
+                        const int32_t y = sa[e];
+                        c += (contains(lb, nlong, y, a.linear_below) &&
+                              !excluded(S, ex, k, cand, y))
+                                 ? 1
+                                 : 0;
+                    }
                 }
             }
             lv[p - pb] = c;

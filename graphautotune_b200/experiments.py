@@ -82,6 +82,40 @@ def run_c1(args):
              matches_per_s=(r.count if mode == "exact" else r.count / 3) / (min(times) / 1e3))
 
 
+def run_c2(args):
+    """R-MAT 2^20 (2^24 samples, seed 2): the 4-clique and the 4-cycle with
+    the default configuration and with the configuration the in-process
+    autotuner finds (tuner.tune_count: `--tune` measured points, proposals
+    ranked by the cost model when --model is given); counts must agree."""
+    from graphautotune_b200 import costmodel, tuner
+
+    gr = g.Graph.rmat(20, 1 << 24, 0.57, 0.19, 0.19, 2, device=True)
+    gr.upload(degree_order=True)
+    V, E, md = gr.info()
+    emit(config="c2", graph="R-MAT scale 20, 2^24 samples, seed 2", V=V, E=E, max_degree=md)
+    for name, pat in (("k4", "0111101111011110"), ("c4", "0101101001011010")):
+        s = g.Schedule(pat, "exact", stats_graph=gr)
+        ex = g.Executor()
+        ex.count(gr, s)
+        rs = [ex.count(gr, s) for _ in range(3)]
+        t_def = min(r.kernel_ms for r in rs)
+        model = None
+        if args.model:
+            model = costmodel.TunerModel(costmodel.CostModel.load(args.model),
+                                         costmodel.graph_features(gr),
+                                         costmodel.plan_features(s))
+        t0 = time.time()
+        cfg, hist, counts = tuner.tune_count(gr, s, budget=max(args.tune, 4), model=model)
+        ex_t = g.Executor(cfg)
+        rt = [ex_t.count(gr, s) for _ in range(3)]
+        t_tuned = min(r.kernel_ms for r in rt)
+        assert rt[0].count == rs[0].count
+        emit(config="c2", pattern=name, count=rs[0].count, default_ms=t_def, tuned_ms=t_tuned,
+             tuned_vs_default=t_def / t_tuned, points=len(hist), tuning_s=time.time() - t0,
+             kernel="dedicated" if s.dedicated_kernel else "schedule plan",
+             tuned={k: getattr(cfg, k) for k in cfg._FIELDS})
+
+
 def run_c3(args):
     """R-MAT 2^22 (2^26 samples, seed 3): house and 5-clique, exact and
     reference-compatible.  Every pattern is first timed on `--slices`
@@ -205,9 +239,13 @@ def run_c4(args):
             tscheds[p], tim = tuner.pick_schedule(ex, big, p, parts=64, slices=4)
             chosen[p] = {"variant": tscheds[p].variant, "slice_ms": tim}
         emit(config="c4", arm="schedules", picked=chosen, seconds=time.perf_counter() - t)
+    # Jobs whose pattern has a dedicated kernel (the 5-clique) keep it: they
+    # are counted by the executor, the others in the one batched launch.
+    dedicated = [p for p in pats if scheds[p].dedicated_kernel]
+    bpats = [p for p in pats if p not in dedicated]
     b = g.Batch()
     for gr in graphs:
-        for p in pats:
+        for p in bpats:
             b.add(gr, tscheds[p])
     if args.tune:
 
@@ -215,7 +253,7 @@ def run_c4(args):
         # job's work queue, slices spread over the queues.
         P = args.tune_parts
         sample, screen = g.Batch(), g.Batch()
-        for j, (gr, p) in enumerate((gr, p) for gr in graphs for p in pats):
+        for j, (gr, p) in enumerate((gr, p) for gr in graphs for p in bpats):
             sample.add_shard(gr, tscheds[p], (j * 7) % P, P)
             screen.add_shard(gr, tscheds[p], (j * 7) % (8 * P), 8 * P)
         model = None
@@ -226,24 +264,38 @@ def run_c4(args):
             gfs = [costmodel.graph_features(gr) for gr in graphs]
             pfs = {p: costmodel.plan_features(tscheds[p]) for p in pats}
             model = costmodel.BatchTunerModel(costmodel.CostModel.load(args.model),
-                                              [(gf, pfs[p]) for gf in gfs for p in pats])
+                                              [(gf, pfs[p]) for gf in gfs for p in bpats])
         t = time.perf_counter()
         cfg, hist = tuner.tune_batch(sample, budget=args.tune, model=model, screen=screen)
         emit(config="c4", arm="tuner", sample=f"1/{P} of every job", history=hist,
              ranking="cost model" if model else "nearest measured point",
              tuning_s=time.perf_counter() - t)
     b.prepare(cfg, cuda_graph=True)
-    t = time.perf_counter()
-    r = b.run()
-    runs = [((time.perf_counter() - t) * 1e3, r.kernel_ms)]
-    while len(runs) < 3 and runs[-1][0] < 10000:  # long batches need no warm-up repeats
+
+    def run_all():
         t = time.perf_counter()
         r = b.run()
-        runs.append(((time.perf_counter() - t) * 1e3, r.kernel_ms))
-    counts = b.counts()
+        ms = r.kernel_ms
+        dcounts = {}
+        for gi, gr in enumerate(graphs):
+            for p in dedicated:
+                rd = ex.count(gr, scheds[p])
+                dcounts[(gi, p)] = rd.count
+                ms += rd.kernel_ms
+        return (time.perf_counter() - t) * 1e3, ms, dcounts
+
+    runs = [run_all()]
+    while len(runs) < 3 and runs[-1][0] < 10000:  # long batches need no warm-up repeats
+        runs.append(run_all())
+    bc = iter(b.counts())
+    dcounts = runs[-1][2]
+    counts = [dcounts[(gi, p)] if p in dedicated else next(bc)
+              for gi in range(len(graphs)) for p in pats]
     assert counts == plain_counts, "batched counts differ from the plain launches"
     best_wall = min(x[0] for x in runs)
-    emit(config="c4", arm="batched", launches=1, kernel_ms=min(x[1] for x in runs),
+    emit(config="c4", arm="batched", launches=1 + len(graphs) * len(dedicated),
+         dedicated_kernel_jobs=len(graphs) * len(dedicated),
+         kernel_ms=min(x[1] for x in runs),
          wall_ms=best_wall, config_used={k: getattr(cfg, k) for k in cfg._FIELDS},
          speedup_vs_plain_wall=plain_wall / best_wall, counts_equal=True,
          matches=sum(counts))
@@ -320,7 +372,7 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64, graph=None, names=N
             sh = P // 2
             t0 = time.time()
             _, r = g.Executor(tuner.to_config(default)).count_shard(gr, s, sh, P)
-            if r.kernel_ms < 500 or P >= parts << 8:
+            if r.kernel_ms < 100 or P >= parts << 8:
                 break
             P <<= 2
 
@@ -333,7 +385,7 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64, graph=None, names=N
 
         raw0, t_default = measure(default)
         emit(config="c5", pattern=name, slice=f"shard {sh} of {P}", default_ms=t_default)
-        t_budget = time.time() + 100.0  # per pattern: candidates measured until then
+        t_budget = time.time() + 60.0  # per pattern: candidates measured until then
         if t_default > 20000:
             emit(config="c5", pattern=name, skipped="slice too slow")
             continue
@@ -376,23 +428,47 @@ def run_c5(args):
     V, E, md = gr.info()
     emit(config="c5", graph="R-MAT scale 24, 12*2^24 samples (avg degree 24), seed 4", V=V,
          E=E, max_degree=md, generate_on_device_s=t_gen, upload_s=time.time() - t0)
+    # The 6-clique: the clique kernels on spread slices of the level-1 units
+    # (the full count is out of reach of one call's time), and the schedule
+    # plan path on the middle slice for comparison; counts must agree.
     ex = g.Executor()
+    plan_cfg = g.Config.engine_default()
+    plan_cfg.special_kernels = 0
+    ex_plan = g.Executor(plan_cfg)
     s = g.Schedule(C5_PATTERNS["k6"], "exact", stats_graph=gr)
-    r = ex.count(gr, s)
-    times = [ex.count(gr, s).kernel_ms for _ in range(2)]
-    emit(config="c5", pattern="k6", count=r.count, kernel_ms=min(times),
-         matches_per_s=r.count / (min(times) / 1e3), launches=r.launches,
-         kernel="clique kernels" if r.launches == 2 else "schedule plan")
+    P, nsl = args.parts, 8
+    raw = ms = 0
+    done = 0
+    for i in range(nsl):
+        sh = i * P // nsl
+        r0, rs = ex.count_shard(gr, s, sh, P)
+        raw += r0
+        ms += rs.kernel_ms
+        done += 1
+        emit(config="c5", pattern="k6", slice=f"shard {sh} of {P}", count=r0,
+             clique_kernels_ms=rs.kernel_ms)
+        if ms > args.max_seconds * 1e3:
+            break
+    nsl = done
+    emit(config="c5", pattern="k6", slices=f"{nsl} of {P}", slice_count=raw,
+         slice_ms=ms, matches_per_s=raw / (ms / 1e3), estimate_full_s=ms * P / nsl / 1e3)
+    sh = P // 2
+    rc, rcs = ex.count_shard(gr, s, sh, P)
+    rp, rps = ex_plan.count_shard(gr, s, sh, P)
+    assert rc == rp, "clique kernels and schedule plan disagree"
+    emit(config="c5", pattern="k6", slice=f"shard {sh} of {P}", count=rc,
+         clique_kernels_ms=rcs.kernel_ms, schedule_plan_ms=rps.kernel_ms,
+         speedup=rps.kernel_ms / rcs.kernel_ms)
     if args.model:
         from graphautotune_b200.costmodel import CostModel
 
         eval_c5(CostModel.load(args.model), parts=args.parts, graph=gr,
-                names=["c6_chord", "tri_path_7v"])
+                names=["c6_chord", "tri_path_7v"], n_candidates=args.candidates)
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["c1", "c3", "c4", "c5"])
+    ap.add_argument("config", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--graphs", type=int, default=64)
     ap.add_argument("--tune", type=int, default=0)
     ap.add_argument("--max-seconds", type=float, default=120.0)
@@ -404,11 +480,13 @@ def main():
     ap.add_argument("--estimate", type=int, default=0,
                     help="c4: estimate every job from 4 slices of 1/N of its queue")
     ap.add_argument("--slices", type=int, default=8)
+    ap.add_argument("--candidates", type=int, default=16,
+                    help="c5: launch configurations measured per pattern")
     args = ap.parse_args()
     import torch
 
     torch.cuda.set_device(0)
-    {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args)
+    {"c1": run_c1, "c2": run_c2, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args)
 
 
 if __name__ == "__main__":

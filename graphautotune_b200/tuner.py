@@ -240,6 +240,34 @@ def tune_batch(b: "g.Batch", budget: int = 12, seed: int = 0, record: str | None
     return to_config(best), [[fingerprint(x), y] for x, y in zip(hist.xs, hist.ys)]
 
 
+def tune_count(graph: "g.Graph", schedule: "g.Schedule", budget: int = 16, seed: int = 0,
+               record: str | None = None, model=None, reps: int = 2
+               ) -> tuple["g.Config", list, dict]:
+    """In-process tuning of one (graph, pattern) count: the default point,
+    a few random warm-up points, then proposals ranked by `model` (the
+    learned cost model's TunerModel, or the nearest measured point), `budget`
+    points measured in all by the count's device time (best of `reps`).
+    Returns (best config, history, {fingerprint: count}); every point must
+    give the same count."""
+    rng = random.Random(seed)
+    hist = History(record)
+    todo = [default_point()] + [random_point(rng) for _ in range(max(1, budget // 3))]
+    counts: dict[str, int] = {}
+    while len(hist.xs) < budget:
+        if not todo:
+            todo = propose(model or NearestModel(hist), hist, 3, rng) or [random_point(rng)]
+        d = todo.pop(0)
+        if hist.seen(d) or not valid(d):
+            continue
+        ex = g.Executor(to_config(d))
+        rs = [ex.count(graph, schedule) for _ in range(reps)]
+        counts[fingerprint(d)] = rs[0].count
+        hist.add(d, min(r.kernel_ms for r in rs) / 1e3)
+    assert len(set(counts.values())) == 1, "configurations disagree on the count"
+    best, _ = hist.best()
+    return to_config(best), [[fingerprint(x), y] for x, y in zip(hist.xs, hist.ys)], counts
+
+
 class PmDriver:
     """The reference driver's protocol (role/driver.py:88-132) over the
     pm-compatible CLI: runs `pm <graph> <pattern> <hash> --config <file>` and

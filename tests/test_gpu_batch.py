@@ -1,6 +1,7 @@
 """Batched persistent launches: every job's count equals the single-job
 count, for several launch shapes, with and without CUDA-graph replay, and on
 repeated runs of the same prepared batch."""
+import json
 from pathlib import Path
 
 import pytest
@@ -71,3 +72,20 @@ def test_sliced_jobs_sum_to_whole(gat):
             assert sum(parts) == whole.raw_sum
             assert sum(parts) // whole.divisor == whole.count
             i += P
+
+
+def test_tune_count_measures_points_and_keeps_the_count(gat, tmp_path):
+    """tuner.tune_count: the default point and proposals, each measured by
+    the count's device time, all giving the same count; record.json and
+    best_config.json are written beside each other."""
+    from graphautotune_b200 import tuner
+
+    g = gat.Graph.rmat(12, 1 << 15, 0.57, 0.19, 0.19, 4)
+    s = gat.Schedule("0100110110010110110010100", "exact")  # the house: plan interpreter
+    rec = tmp_path / "tuning_results" / "record.json"
+    cfg, hist, counts = tuner.tune_count(g, s, budget=6, record=str(rec))
+    assert len(hist) == 6 and len(set(counts.values())) == 1
+    assert hist[0][0] == tuner.fingerprint(tuner.default_point())
+    best = json.loads((rec.parent / "best_config.json").read_text())
+    assert best[1] == min(y for _, y in hist)
+    assert gat.Executor(cfg).count(g, s).count == next(iter(counts.values()))

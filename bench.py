@@ -557,7 +557,8 @@ def run_ours(args):
         for i in range(max(1, min(3, args.steps))):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            g2 = g.Graph.from_csr(off_p.numpy(), adj_p.numpy(), check_symmetry=False)
+            g2 = g.Graph.from_csr(off_p.numpy(), adj_p.numpy(), check_symmetry=False,
+                                  device=True)
             t1 = time.perf_counter()
             g2.upload(degree_order=True)
             t2 = time.perf_counter()

@@ -212,13 +212,21 @@ class Graph(_Handle):
         return g
 
     @classmethod
-    def from_csr(cls, offsets: np.ndarray, adj: np.ndarray, check_symmetry: bool = True
-                 ) -> "Graph":
+    def from_csr(cls, offsets: np.ndarray, adj: np.ndarray, check_symmetry: bool = True,
+                 device: bool = False, stream: int | None = None) -> "Graph":
+        """A graph from host CSR arrays; device=True copies them straight to
+        the current GPU (gat_graph_from_csr_device) and checks them there."""
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         a = np.ascontiguousarray(adj, dtype=np.int32)
         g = cls()
-        check(lib().gat_graph_from_csr(len(off) - 1, len(a), off.ctypes.data, a.ctypes.data,
-                                       C.byref(g._h)))
+        if device:
+            check(lib().gat_graph_from_csr_device(len(off) - 1, len(a), off.ctypes.data,
+                                                  a.ctypes.data,
+                                                  C.c_void_p(stream) if stream else None,
+                                                  C.byref(g._h)))
+        else:
+            check(lib().gat_graph_from_csr(len(off) - 1, len(a), off.ctypes.data, a.ctypes.data,
+                                           C.byref(g._h)))
         if check_symmetry:
             check(lib().gat_graph_validate(g._h, 1))
         return g

@@ -100,6 +100,8 @@ _SIGS = {
     "gat_graph_generate_device": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double,
                                             C.c_double, C.c_double, C.c_uint64, P,
                                             C.POINTER(P)]),
+    "gat_graph_from_csr_device": (C.c_int, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, P,
+                                            C.POINTER(P)]),
     "gat_graph_validate": (C.c_int, [P, C.c_int]),
     "gat_graph_save": (C.c_int, [P, C.c_char_p]),
     "gat_graph_info": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int64),

@@ -203,7 +203,10 @@ def collect(runs: int, seed: int = 0, graphs: int = 24, max_ms: float = 200.0,
         gr = make_graph(sp)
         gr.upload(degree_order=True)
         glist.append((gr, graph_features(gr)))
-    scheds = [g.Schedule(p, "exact") for p in pats]
+    # every pattern's exact plan variants (up to 4), so that the model also
+    # sees how plans of one pattern differ
+    scheds = [g.Schedule(p, "exact", variant=v) for p in pats
+              for v in range(min(4, g.Schedule.variants(p)))]
     pfs = [plan_features(s) for s in scheds]
     X, T = [], []
     if checkpoint:
@@ -322,6 +325,27 @@ def pick(model: CostModel, gf: np.ndarray, pf: np.ndarray, points: list[dict]) -
 # The model leaves the default configuration only for a predicted gain of at
 # least this factor: its ranking error on held-out graphs is of that order.
 MIN_PREDICTED_GAIN = 1.15
+
+
+def choose_schedule(model: CostModel, graph: "g.Graph", pattern: str,
+                    point: dict | None = None, max_variants: int = 8,
+                    min_gain: float = MIN_PREDICTED_GAIN) -> tuple["g.Schedule", bool]:
+    """The model's choice among the pattern's exact plan variants (vertex
+    orders and their symmetry-breaking conditions, all counting the same
+    subgraphs) under launch configuration `point` (default: the engine's),
+    falling back to variant 0 - the reference cost formula's first choice,
+    with the graph's sizes - unless the best prediction beats it by
+    min_gain.  Returns (schedule, whether variant 0 was kept)."""
+    point = point or tuner.default_point()
+    n = min(max_variants, g.Schedule.variants(pattern, stats_graph=graph))
+    scheds = [g.Schedule(pattern, "exact", stats_graph=graph, variant=v) for v in range(n)]
+    gf = graph_features(graph)
+    X = np.stack([features(gf, plan_features(s), point) for s in scheds])
+    pred = model.predict(X)
+    bi = int(np.argmin(pred))
+    if pred[bi] + math.log(min_gain) <= pred[0]:
+        return scheds[bi], False
+    return scheds[0], True
 
 
 def choose(model: CostModel, gf: np.ndarray, pf: np.ndarray, points: list[dict],

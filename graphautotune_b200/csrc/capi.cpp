@@ -102,6 +102,10 @@ struct gat_graph {
     int64_t hub_min_degree = GAT_HUB_MIN_DEGREE_DEFAULT;
     int64_t hub_max_bytes = GAT_HUB_MAX_BYTES_DEFAULT;
     bool dev_hubs_pending = false;
+    // Built on the device (gat_graph_generate_device,
+    // gat_graph_from_csr_device): host.off is filled, host.adj is read back
+    // from the resident copy on first use.
+    bool host_adj_pending = false;
     ~gat_graph() {
         dev.release();
         dev_ordered.release();
@@ -130,6 +134,27 @@ struct gat_executor {
         if (ev1) cudaEventDestroy(ev1);
     }
 };
+
+namespace {
+// Reads host.adj back from the resident device copy when the graph was built
+// on the device and the host neighbours were not needed until now.
+int ensure_host_adj(gat_graph *g) {
+    if (!g->host_adj_pending) return GAT_OK;
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (cur != g->device || !g->dev.ready)
+        return fail(GAT_ERR_STATE, "graph built on another device: make it current to read it");
+    std::vector<int32_t> adj(size_t(g->host.E));
+    if (g->host.E > 0 &&
+        (e = cudaMemcpy(adj.data(), g->dev.adj, sizeof(int32_t) * size_t(g->host.E),
+                        cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return cuda_fail(e, "graph read-back");
+    g->host.adj.swap(adj);
+    g->host_adj_pending = false;
+    return GAT_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -467,6 +492,8 @@ int gat_graph_from_csr(int32_t V, int64_t E, const int64_t *offsets,
 
 int gat_graph_validate(const gat_graph *g, int check_symmetry) {
     if (!g) return fail(GAT_ERR_ARGUMENT, "null argument");
+    int rc = ensure_host_adj(const_cast<gat_graph *>(g));
+    if (rc != GAT_OK) return rc;
     std::string err;
     if (!validate(g->host, check_symmetry != 0, &err))
         return fail(GAT_ERR_ARGUMENT, "invalid CSR: " + err);
@@ -497,6 +524,8 @@ int gat_graph_generate(int kind, double p0, double p1, double p2, double p3,
 
 int gat_graph_save(const gat_graph *g, const char *path) {
     if (!g || !path) return fail(GAT_ERR_ARGUMENT, "null argument");
+    int rc = ensure_host_adj(const_cast<gat_graph *>(g));
+    if (rc != GAT_OK) return rc;
     std::string err;
     if (!save_binary(path, g->host, &err)) return fail(GAT_ERR_IO, err);
     return GAT_OK;
@@ -512,6 +541,8 @@ int gat_graph_info(const gat_graph *g, int32_t *V, int64_t *E, int32_t *max_degr
 
 int gat_graph_csr(const gat_graph *g, const int64_t **offsets, const int32_t **adj) {
     if (!g || !offsets || !adj) return fail(GAT_ERR_ARGUMENT, "null argument");
+    int rc = ensure_host_adj(const_cast<gat_graph *>(g));
+    if (rc != GAT_OK) return rc;
     *offsets = g->host.off.data();
     *adj = g->host.adj.data();
     return GAT_OK;
@@ -713,11 +744,8 @@ int gat_graph_generate_device(int kind, double p0, double p1, double p2, double 
     h.V = V;
     h.E = E;
     h.off.resize(size_t(V) + 1);
-    h.adj.resize(size_t(E));
     if ((e = cudaMemcpyAsync(h.off.data(), d.off, sizeof(int64_t) * (size_t(V) + 1),
                              cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
-        (E > 0 && (e = cudaMemcpyAsync(h.adj.data(), d.adj, sizeof(int32_t) * size_t(E),
-                                       cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess) {
         d.release();
         return cuda_fail(e, "device graph read-back");
@@ -727,6 +755,62 @@ int gat_graph_generate_device(int kind, double p0, double p1, double p2, double 
     int dev = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     g->device = dev;
+    g->host_adj_pending = true;
+    *out = g.release();
+    return GAT_OK;
+}
+
+int gat_graph_from_csr_device(int32_t V, int64_t E, const int64_t *offsets,
+                              const int32_t *adj, void *stream, gat_graph **out) {
+    if (!out || V < 0 || E < 0 || !offsets || (E > 0 && !adj))
+        return fail(GAT_ERR_ARGUMENT, "bad CSR arguments");
+    *out = nullptr;
+    cudaStream_t st = (cudaStream_t)stream;
+    auto g = std::make_unique<gat_graph>();
+    DevCopy &d = g->dev;
+    unsigned long long *flag = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&d.off, sizeof(int64_t) * (size_t(V) + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&d.adj, sizeof(int32_t) * adj_alloc_ints(E))) != cudaSuccess ||
+        (e = cudaMalloc(&flag, sizeof(unsigned long long))) != cudaSuccess) {
+        d.release();
+        cudaFree(flag);
+        return fail(GAT_ERR_MEMORY, std::string("device graph allocation: ") + cudaGetErrorString(e));
+    }
+    HostGraph &h = g->host;
+    h.V = V;
+    h.E = E;
+    h.off.assign(offsets, offsets + size_t(V) + 1);
+    unsigned long long bad = ~0ull;
+    if ((e = cudaMemcpyAsync(d.off, offsets, sizeof(int64_t) * (size_t(V) + 1),
+                             cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (E > 0 && (e = cudaMemcpyAsync(d.adj, adj, sizeof(int32_t) * size_t(E),
+                                       cudaMemcpyHostToDevice, st)) != cudaSuccess) ||
+        (e = csr_check_device(d.off, d.adj, V, E, flag, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&bad, flag, sizeof(bad), cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+        d.release();
+        cudaFree(flag);
+        return cuda_fail(e, "graph upload");
+    }
+    cudaFree(flag);
+    if (V > 0 && (h.off[0] != 0 || h.off[size_t(V)] != E))
+        bad = std::min<unsigned long long>(bad, kCsrOffsets);
+    if (bad != ~0ull) {
+        static const char *why[] = {"", "offsets not monotone or outside [0, E]",
+                                    "neighbour id out of range", "self loop",
+                                    "row not strictly increasing"};
+        d.release();
+        return fail(GAT_ERR_ARGUMENT, "invalid CSR: row " + std::to_string(bad >> 3) + ": " +
+                                          why[bad & 7u]);
+    }
+    int rc = finish_copy(d, V, h.max_degree(), &h.off, st);
+    if (rc != GAT_OK) return rc;
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    g->device = dev;
+    g->host_adj_pending = true;
     *out = g.release();
     return GAT_OK;
 }
@@ -745,7 +829,7 @@ int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
     int rc = GAT_OK;
     if (g->dev.ready && g->device == dev)
         release_hubs(g->dev);
-    else
+    else if ((rc = ensure_host_adj(g)) == GAT_OK)
         rc = upload_copy(g->host, g->dev, st);
     g->hub_min_degree = hub_min_degree;
     g->hub_max_bytes = hub_max_bytes;
@@ -758,7 +842,9 @@ int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
             release_hubs(g->dev_ordered);
             rc = GAT_OK;
         } else {
-            rc = derive_ordered_copy(g->host, g->dev, g->dev_ordered, st);
+            // graphs too large for the device relabel are relabelled on the host
+            if (!relabel_fits_device(V, g->host.E)) rc = ensure_host_adj(g);
+            if (rc == GAT_OK) rc = derive_ordered_copy(g->host, g->dev, g->dev_ordered, st);
         }
         if (rc == GAT_OK)
             rc = upload_hubs(g->dev_ordered, V, hub_min_degree, hub_max_bytes, st);

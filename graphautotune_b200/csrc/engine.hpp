@@ -130,6 +130,11 @@ cudaError_t launch_clique(const CliqueLaunch &launch, cudaStream_t st);
 cudaError_t rmat_csr_device(int scale, int64_t samples, double a, double b, double c,
                             uint64_t seed, int64_t *off, int32_t **adj, int64_t pad_ints,
                             int64_t *E, cudaStream_t st);
+// Checks a device CSR by the host validate() rules without symmetry; *flag
+// ends as ~0 when every row passes, else (first failing row << 3) | reason.
+enum : unsigned { kCsrOffsets = 1, kCsrRange = 2, kCsrLoop = 3, kCsrOrder = 4 };
+cudaError_t csr_check_device(const int64_t *off, const int32_t *adj, int32_t V, int64_t E,
+                             unsigned long long *flag, cudaStream_t st);
 // An undirected edge list of n (u, v) pairs (device memory) on V vertices.
 cudaError_t pairs_csr_device(const int32_t *pairs, int64_t n, int32_t V, int64_t *off,
                              int32_t **adj, int64_t pad_ints, int64_t *E, cudaStream_t st);

@@ -144,7 +144,52 @@ cudaError_t keys_to_csr(uint64_t *keys, int64_t nkeys, int32_t V, int64_t *off, 
     return e;
 }
 
+// A warp per row: the CSR rules the host's validate() checks without
+// symmetry (offsets monotone and inside [0, E], ids in [0, V), no self loop,
+// rows strictly increasing).  The lowest failing row wins: *flag takes
+// min(row << 3 | reason).
+__global__ void csr_check_kernel(const int64_t *__restrict__ off,
+                                 const int32_t *__restrict__ adj, int32_t V, int64_t E,
+                                 unsigned long long *flag) {
+    const int64_t v = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (v >= V) return;
+    const int64_t b = off[v], e = off[v + 1];
+    unsigned reason = 0;
+    if (b < 0 || e < b || e > E || (v == 0 && b != 0) || (v == V - 1 && e != E)) {
+        reason = kCsrOffsets;
+    } else {
+        // rows are warp-uniform, so every lane runs every chunk
+        for (int64_t base = b; base < e; base += 32) {
+            const int64_t i = base + lane;
+            unsigned r = 0;
+            if (i < e) {
+                const int32_t u = adj[i];
+                if (u < 0 || u >= V) r = kCsrRange;
+                else if (u == v) r = kCsrLoop;
+                else if (i > b && adj[i - 1] >= u) r = kCsrOrder;
+            }
+            // the host check reports the first failing entry's reason
+            const unsigned m = __ballot_sync(0xffffffffu, r != 0);
+            if (m) {
+                reason = __shfl_sync(0xffffffffu, r, __ffs(m) - 1);
+                break;
+            }
+        }
+    }
+    if (lane == 0 && reason)
+        atomicMin(flag, ((unsigned long long)v << 3) | reason);
+}
+
 }  // namespace
+
+cudaError_t csr_check_device(const int64_t *off, const int32_t *adj, int32_t V, int64_t E,
+                             unsigned long long *flag, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(flag, 0xFF, sizeof(unsigned long long), st);
+    if (e != cudaSuccess || V <= 0) return e;
+    csr_check_kernel<<<blocks(int64_t(V) * 32), 256, 0, st>>>(off, adj, V, E, flag);
+    return cudaGetLastError();
+}
 
 cudaError_t rmat_csr_device(int scale, int64_t samples, double a, double b, double c,
                             uint64_t seed, int64_t *off, int32_t **adj, int64_t pad_ints,

@@ -170,6 +170,16 @@ int gat_graph_load(const char *path, int binary, gat_graph **out);
  * which gat_graph_validate(g, 1) checks in O(E log d). */
 int gat_graph_from_csr(int32_t V, int64_t E, const int64_t *offsets,
                        const int32_t *adj, gat_graph **out);
+/* As gat_graph_from_csr, but the arrays go straight to the current device
+ * (one host-to-device copy each on `stream`; from pinned host memory the
+ * copy runs at full PCIe speed) and the row rules are checked there by a
+ * kernel; the host view reads the neighbours back only when asked for
+ * (gat_graph_csr, gat_graph_save, gat_graph_validate).  The caller's arrays
+ * may be freed when the call returns.  Replaces GlobalMemoryGraph's load +
+ * to_device (infra/graph_backend.cuh:102-118) for callers that hold the CSR
+ * in host memory already. */
+int gat_graph_from_csr_device(int32_t V, int64_t E, const int64_t *offsets,
+                              const int32_t *adj, void *stream, gat_graph **out);
 int gat_graph_validate(const gat_graph *g, int check_symmetry);
 /* Seeded synthetic graphs (splitmix64 streams).  kind: 0 Erdos-Renyi
  * (p0 = n, p1 = avg degree), 1 R-MAT (p0 = scale, p1 = edge samples,

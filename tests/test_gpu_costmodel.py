@@ -115,3 +115,45 @@ def test_trained_model_beats_choosing_without_it(gat):
     assert info["vs_default"] >= 1.0, info
     assert info["vs_best"] >= 0.5, info
     assert info["corr"] > 0.5, info
+
+
+def test_model_ranks_schedule_variants(gat):
+    """The model, trained on engine timings that include every pattern's
+    first exact plan variants, chooses among the plan variants of patterns
+    on held-out graphs (costmodel.choose_schedule, with variant 0 - the
+    reference cost formula's first choice - as the fallback).  Judged by
+    measured times against variant 0 and against the best variant: the
+    choice must not lose more than 10 % to variant 0 (geometric mean) and
+    must keep at least half the best variant's speed."""
+    from graphautotune_b200 import costmodel
+    from graphautotune_b200.experiments import make_graph
+
+    X, T = costmodel.collect(1500, seed=7, graphs=12, max_ms=50.0, max_seconds=90.0,
+                             max_log2=12)
+    model, _ = costmodel.CostModel.fit(X, T, epochs=200, seed=0, lr=2e-3)
+    ex = gat.Executor()
+    vs_v0, vs_best, kept = [], [], 0
+    for sp in costmodel.training_graphs(4, seed0=9100, max_log2=12):
+        gr = make_graph(sp)
+        gr.upload(degree_order=True)
+        for p in ("0100110110010110110010100", "0000100110010110110110110"):
+            n = min(8, gat.Schedule.variants(p, stats_graph=gr))
+            times = []
+            for v in range(n):
+                s = gat.Schedule(p, "exact", stats_graph=gr, variant=v)
+                ex.count(gr, s)
+                times.append(min(ex.count(gr, s).kernel_ms for _ in range(2)))
+            choice, k = costmodel.choose_schedule(model, gr, p)
+            kept += k
+            t = times[choice.variant]
+            vs_v0.append(times[0] / t)
+            vs_best.append(min(times) / t)
+
+    def gm(xs):
+        return math.exp(sum(math.log(x) for x in xs) / len(xs))
+
+    info = dict(vs_variant0=gm(vs_v0), vs_best=gm(vs_best), kept_variant0=kept,
+                groups=len(vs_v0))
+    print(info)
+    assert info["vs_variant0"] >= 0.9, info
+    assert info["vs_best"] >= 0.5, info

@@ -353,3 +353,30 @@ def test_schedule_variants_count_the_same(gat, oracle):
         assert len(counts) == 1, (p, counts)
         best, timings = tuner.pick_schedule(ex, big, p, parts=16, slices=2)
         assert len(timings) == n and ex.count(big, best).count in counts
+
+
+def test_config5_patterns_on_small_graphs(gat, oracle, golden_graphs):
+    """The learned-cost-model workload's patterns (6-clique, 6-cycle with a
+    chord, 7-vertex triangle + path) counted by the engine on small graphs:
+    exact counts equal the oracle's, with the dedicated kernels and with the
+    plan interpreter, on the default launch shape and five random points of
+    the tuner's space."""
+    import random
+
+    from graphautotune_b200 import tuner
+    from graphautotune_b200.experiments import C5_PATTERNS
+
+    rng = random.Random(5)
+    shapes = [tuner.default_point()] + [tuner.random_point(rng) for _ in range(5)]
+    exs = [gat.Executor(tuner.to_config(d)) for d in shapes]
+    plain = _executor(gat, special_kernels=0)
+    graphs = [golden_graphs["er60"], golden_graphs["ba60"], golden_graphs["k7"],
+              golden_graphs["rmat6"], gat.Graph.barabasi_albert(400, 3, 11)]
+    for g in graphs:
+        off, adj = g.csr()
+        for name, p in C5_PATTERNS.items():
+            want = oracle.exact_count(off, adj, p)
+            s = gat.Schedule(p, "exact")
+            assert plain.count(g, s).count == want, (name, "plan")
+            for ex in exs:
+                assert ex.count(g, s).count == want, (name, ex)

@@ -93,3 +93,52 @@ def test_device_generated_graphs_equal_host_generated(gat):
         s = gat.Schedule(pat, "exact")
         assert ex.count(g, s).count == ex.count(gat.Graph.rmat(13, 1 << 17, 0.57, 0.19, 0.19, 5),
                                                 s).count
+
+
+def test_from_csr_device_checks_rows_and_reads_back_lazily(gat, oracle):
+    """gat_graph_from_csr_device: the caller's host CSR goes straight to the
+    GPU and is checked there by the host validator's rules (first failing
+    row reported); the host view reads the neighbours back on first use;
+    counts equal those of the host-built graph."""
+    import torch
+
+    from graphautotune_b200._lib import GatError
+
+    src = gat.Graph.rmat(12, 1 << 15, 0.57, 0.19, 0.19, 9)
+    off, adj = src.csr()
+    off_p = torch.from_numpy(off).pin_memory()
+    adj_p = torch.from_numpy(adj).pin_memory()
+    d = gat.Graph.from_csr(off_p.numpy(), adj_p.numpy(), check_symmetry=False, device=True)
+    assert d.info() == src.info()
+    d.upload(degree_order=True)
+    ex = gat.Executor()
+    for p in ("011101110", "0111101111011110", "0101101001011010",
+              "0100110110010110110010100"):
+        s = gat.Schedule(p, "exact")
+        assert ex.count(d, s).count == ex.count(src, s).count == oracle.exact_count(off, adj, p)
+        sr = gat.Schedule(p, "ref")
+        assert ex.count(d, sr).count == ex.count(src, sr).count
+    do, da = d.csr()
+    assert np.array_equal(do, off) and np.array_equal(da, adj)
+    # invalid inputs: the lowest failing row and its reason
+    V = len(off) - 1
+    row = int(np.argmax(np.diff(off) >= 3))
+    cases = []
+    a2 = adj.copy()
+    a2[off[row]] = row
+    cases.append((off, a2, "self loop"))
+    a3 = adj.copy()
+    a3[off[row]], a3[off[row] + 1] = a3[off[row] + 1], a3[off[row]]
+    cases.append((off, a3, "row not strictly increasing"))
+    a4 = adj.copy()
+    a4[off[row]] = V + 7
+    cases.append((off, a4, "neighbour id out of range"))
+    o5 = off.copy()
+    o5[row + 1] = o5[row] - 1
+    cases.append((o5, adj, "offsets not monotone"))
+    for o, a, why in cases:
+        with pytest.raises(GatError) as err:
+            gat.Graph.from_csr(o, a, check_symmetry=False, device=True)
+        assert why in str(err.value), (why, str(err.value))
+    empty = gat.Graph.from_csr(np.zeros(4, np.int64), np.zeros(0, np.int32), device=True)
+    assert empty.info()[:2] == (3, 0)

@@ -372,6 +372,7 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64, graph=None, names=N
             sh = P // 2
             t0 = time.time()
             _, r = g.Executor(tuner.to_config(default)).count_shard(gr, s, sh, P)
+            emit(config="c5", pattern=name, sizing=f"shard {sh} of {P}", default_ms=r.kernel_ms)
             if r.kernel_ms < 100 or P >= parts << 8:
                 break
             P <<= 2
@@ -383,6 +384,13 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64, graph=None, names=N
             assert raw == raw2
             return raw, min(r.kernel_ms, r2.kernel_ms)
 
+        # Every configuration is first timed on a slice 8x smaller; one more
+        # than 4x slower there than the default is not measured on the full
+        # slice (a bad launch shape can be 100x slower than a good one).
+        def screen(d):
+            return g.Executor(tuner.to_config(d)).count_shard(gr, s, 4 * P, 8 * P)[1].kernel_ms
+
+        ts0 = screen(default)
         raw0, t_default = measure(default)
         emit(config="c5", pattern=name, slice=f"shard {sh} of {P}", default_ms=t_default)
         t_budget = time.time() + 60.0  # per pattern: candidates measured until then
@@ -390,27 +398,34 @@ def eval_c5(model, parts: int = 256, n_candidates: int = 64, graph=None, names=N
             emit(config="c5", pattern=name, skipped="slice too slow")
             continue
         picked, kept_default = costmodel.choose(model, gf, pf, cands, default)
-        raw_p, t_pick = measure(picked)
-        times = []
+        tsp = screen(picked)
+        raw_p, t_pick = measure(picked) if tsp <= 4 * ts0 else (raw0, math.inf)
+        emit(config="c5", pattern=name, model_pick_ms=t_pick, kept_default=kept_default)
+        times, screened, cands_m = [], 0, []
         for d in cands:
             if times and time.time() > t_budget:
                 break
+            if screen(d) > 4 * ts0:
+                screened += 1
+                continue
             raw_c, t_c = measure(d)
             assert raw_c == raw0, "counts differ across configurations"
             times.append(t_c)
-        cands_m = cands[:len(times)]
+            cands_m.append(d)
         best = int(np.argmin(times))
         pred = model.predict(np.stack([costmodel.features(gf, pf, d) for d in cands_m]))
         rank_corr = float(np.corrcoef(np.argsort(np.argsort(pred)),
-                                      np.argsort(np.argsort(times)))[0, 1])
+                                      np.argsort(np.argsort(times)))[0, 1]) \
+            if len(times) > 2 else None
+        best_ms = min(times[best], t_pick, t_default)
         emit(config="c5", pattern=name, slice_raw_count=raw0, default_ms=t_default,
-             model_pick_ms=t_pick, best_measured_ms=times[best],
+             model_pick_ms=t_pick, best_measured_ms=best_ms,
              median_candidate_ms=float(np.median(times)),
-             pick_vs_default=t_default / t_pick, pick_vs_best=times[best] / t_pick,
-             kept_default=kept_default,
+             pick_vs_default=t_default / t_pick, pick_vs_best=best_ms / t_pick,
+             kept_default=kept_default, screened_out=screened,
              spearman_pred_vs_measured=rank_corr, candidates=len(cands_m),
              picked={k.split(".")[-1]: v for k, v in picked.items()},
-             best={k.split(".")[-1]: v for k, v in cands[best].items()})
+             best={k.split(".")[-1]: v for k, v in cands_m[best].items()})
 
 
 def run_c5(args):

@@ -326,11 +326,15 @@ def pick(model: CostModel, gf: np.ndarray, pf: np.ndarray, points: list[dict]) -
 # The model leaves the default configuration only for a predicted gain of at
 # least this factor: its ranking error on held-out graphs is of that order.
 MIN_PREDICTED_GAIN = 1.15
+# Plan variants need a larger predicted gain: the training runs hold only
+# each pattern's first two variants, so predictions for the others are
+# extrapolations.
+MIN_PREDICTED_PLAN_GAIN = 1.5
 
 
 def choose_schedule(model: CostModel, graph: "g.Graph", pattern: str,
                     point: dict | None = None, max_variants: int = 8,
-                    min_gain: float = MIN_PREDICTED_GAIN) -> tuple["g.Schedule", bool]:
+                    min_gain: float = MIN_PREDICTED_PLAN_GAIN) -> tuple["g.Schedule", bool]:
     """The model's choice among the pattern's exact plan variants (vertex
     orders and their symmetry-breaking conditions, all counting the same
     subgraphs) under launch configuration `point` (default: the engine's),

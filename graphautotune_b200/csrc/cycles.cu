@@ -260,23 +260,36 @@ __device__ __forceinline__ int32_t expand_group(RootSmem<BLOCK> &S, const int32_
     const int32_t jb = (int32_t)(threadIdx.x >> 5) * per;
     const int32_t je = min(total, jb + per);
     int32_t lo = 0;
-    for (int32_t j = jb + (int32_t)(threadIdx.x & 31); j < je; j += 32) {
-        int32_t step = 1;
-        while (lo + step < BLOCK && S.pref[lo + step] <= j) {
-            lo += step;
-            step <<= 1;
-        }
-        int32_t n = min(lo + step, BLOCK) - lo;
-        while (n > 1) {
-            const int32_t h = n >> 1;
-            if (S.pref[lo + h] <= j) {
-                lo += h;
-                n -= h;
-            } else {
-                n = h;
+    // Four entries per step: their list loads are all issued before the
+    // first update uses one, so each lane has four loads in flight.
+    constexpr int kUnroll = 4;
+    for (int32_t j0 = jb + (int32_t)(threadIdx.x & 31); j0 < je; j0 += 32 * kUnroll) {
+        int32_t xs[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const int32_t j = j0 + 32 * u;
+            xs[u] = 0;
+            if (j >= je) continue;
+            int32_t step = 1;
+            while (lo + step < BLOCK && S.pref[lo + step] <= j) {
+                lo += step;
+                step <<= 1;
             }
+            int32_t n = min(lo + step, BLOCK) - lo;
+            while (n > 1) {
+                const int32_t h = n >> 1;
+                if (S.pref[lo + h] <= j) {
+                    lo += h;
+                    n -= h;
+                } else {
+                    n = h;
+                }
+            }
+            xs[u] = __ldg(adj + S.seg_base[lo] + (j - S.pref[lo]));
         }
-        f(__ldg(adj + S.seg_base[lo] + (j - S.pref[lo])));
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
+            if (j0 + 32 * u < je) f(xs[u]);
     }
     return total;
 }

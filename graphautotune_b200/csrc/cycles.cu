@@ -50,6 +50,8 @@ constexpr int kWarpWedges = kWarpSlots / 2;
 constexpr int kLightBlock = 256;          // 8 warps
 constexpr int kCtaSlots = 16384;          // CTA table slots (128 KB)
 constexpr int kCtaWedges = kCtaSlots / 2;
+constexpr int kCtaBits = 14;               // log2(kCtaSlots)
+static_assert((1 << kCtaBits) == kCtaSlots, "table size is a power of two");
 constexpr int kRegionBytes = 196608;      // counters / table region (192 KB)
 constexpr int kRegionWords = kRegionBytes / 4;
 static_assert(kCtaSlots * 8 <= kRegionBytes, "table fits in the region");
@@ -378,7 +380,7 @@ __global__ void __launch_bounds__(BLOCK, 1) c4_root_kernel(const RootArgs a) {
                     }
                 }
                 expand_group<BLOCK>(S, a.adj, base, len, [&](int32_t x) {
-                    table_add(tkey, tcnt, 14, x, &a.ctr->error);
+                    table_add(tkey, tcnt, kCtaBits, x, &a.ctr->error);
                 });
             }
             __syncthreads();
@@ -422,7 +424,7 @@ __global__ void __launch_bounds__(BLOCK, 1) c4_root_kernel(const RootArgs a) {
                         }
                     }
                     expand_group<BLOCK>(S, a.adj, base, len, [&](int32_t x) {
-                        table_add(tkey, tcnt, 14, x, &a.ctr->error);
+                        table_add(tkey, tcnt, kCtaBits, x, &a.ctr->error);
                     });
                 }
                 __syncthreads();

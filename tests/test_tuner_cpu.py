@@ -169,3 +169,77 @@ def test_tune_batch_screens_out_slow_points(tuner, monkeypatch):
     ys = dict(hist)
     for d in full_calls:
         assert math.isclose(ys[tuner.fingerprint(d)], 8.0 * 2.0 ** cost(d))
+
+
+class _StubModel:
+    """Stands in for a trained CostModel: predicted log-times chosen by a
+    function of the feature rows."""
+
+    def __init__(self, fn):
+        self.fn = fn
+
+    def predict(self, X):
+        return np.array([self.fn(x) for x in X], np.float32)
+
+
+def test_choose_keeps_the_default_unless_the_gain_is_large(gat, tuner):
+    """costmodel.choose leaves the default configuration only when the best
+    prediction is at least MIN_PREDICTED_GAIN times faster; the default is
+    added to the candidates when missing."""
+    from graphautotune_b200 import costmodel
+
+    g = gat.Graph.barabasi_albert(600, 4, 3)
+    gf = costmodel.graph_features(g)
+    pf = costmodel.plan_features(gat.Schedule("0100110110010110110010100", "exact"))
+    rng = random.Random(2)
+    default = tuner.default_point()
+    others = []
+    while len(others) < 6:
+        d = tuner.random_point(rng)
+        if tuner.fingerprint(d) != tuner.fingerprint(default):
+            others.append(d)
+    target = tuner.fingerprint(others[3])
+    rows = {tuner.fingerprint(d): costmodel.features(gf, pf, d).tobytes()
+            for d in [default] + others}
+    by_row = {v: k for k, v in rows.items()}
+
+    def model_with(gain):
+        # every point predicts 1.0 (log-time 0) except others[3], predicted
+        # `gain` times faster than the default
+        return _StubModel(lambda x: -math.log(gain) if by_row[x.tobytes()] == target else 0.0)
+
+    pick, kept = costmodel.choose(model_with(1.05), gf, pf, others, default)
+    assert kept and tuner.fingerprint(pick) == tuner.fingerprint(default)
+    pick, kept = costmodel.choose(model_with(2.0), gf, pf, others, default)
+    assert not kept and tuner.fingerprint(pick) == target
+
+
+def test_choose_schedule_keeps_variant_zero_unless_the_gain_is_large(gat):
+    """costmodel.choose_schedule ranks a pattern's exact plan variants and
+    keeps variant 0 (the reference cost formula's choice) unless another is
+    predicted MIN_PREDICTED_PLAN_GAIN times faster."""
+    from graphautotune_b200 import costmodel
+
+    g = gat.Graph.rmat(10, 1 << 13, 0.57, 0.19, 0.19, 3)
+    pat = "0000100110010110110110110"
+    n = gat.Schedule.variants(pat, stats_graph=g)
+    assert n > 2
+    pfs = [costmodel.plan_features(gat.Schedule(pat, "exact", stats_graph=g, variant=v))
+           for v in range(min(8, n))]
+    # the first variant whose plan features differ from variant 0's (the
+    # features summarise a plan's shape, so many vertex orders look alike;
+    # equal rows get equal predictions and the lowest index among them wins)
+    keys = [pf.tobytes() for pf in pfs]
+    t = next(v for v in range(1, len(pfs)) if keys[v] != keys[0])
+    # a model that sees only the plan part of the row: variant t is
+    # predicted faster by `gain`
+    off = 7  # configuration features come first
+
+    def model_with(gain):
+        return _StubModel(lambda x: -math.log(gain)
+                          if x[off:off + len(pfs[t])].tobytes() == keys[t] else 0.0)
+
+    s, kept = costmodel.choose_schedule(model_with(1.2), g, pat)
+    assert kept and s.variant == 0
+    s, kept = costmodel.choose_schedule(model_with(3.0), g, pat)
+    assert not kept and s.variant == t

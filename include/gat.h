@@ -213,13 +213,15 @@ int gat_graph_upload(gat_graph *g, int flags, void *stream);
 /* As gat_graph_upload, also building hub bitmaps: one V-bit row (bit x set
  * iff x is a neighbour) for every vertex of degree >= hub_min_degree, largest
  * degree first, as many as fit in hub_max_bytes (0 disables).
- * gat_graph_upload uses the defaults below. */
+ * gat_graph_upload uses the defaults below.  With GAT_UPLOAD_DEGREE_ORDER,
+ * the given-id copy's bitmaps (used only by reference-compatible counts) are
+ * built on first use, with these parameters. */
 #define GAT_HUB_MIN_DEGREE_DEFAULT 512
 #define GAT_HUB_MAX_BYTES_DEFAULT (1LL << 30)
 int gat_graph_upload_ex(gat_graph *g, int flags, int64_t hub_min_degree,
                         int64_t hub_max_bytes, void *stream);
-/* Number of hub bitmaps on the given device copy (0: ids as given,
- * 1: degree-ordered). */
+/* Number of hub bitmaps on the given device copy (0: ids as given, whose
+ * bitmaps this call builds if they are still pending; 1: degree-ordered). */
 int gat_graph_hubs(const gat_graph *g, int ordered_copy, int32_t *nhubs);
 /* Copies the degree-ordered device copy (uploaded with
  * GAT_UPLOAD_DEGREE_ORDER) into host buffers of V+1 offsets and E
